@@ -1,0 +1,310 @@
+/*
+ * mdb200.h — C ABI of libmdb200.so, the B200-native (sm_100a) MD stepping
+ * library for the 2D binary A/B Lennard-Jones system of MD_Simulation_CUDA.
+ *
+ * Plain C types only: pointers, sizes, POD structs. Every function returns an
+ * int status (MDB_OK == 0) and never exits, aborts or traps; the message of
+ * the last failure on the calling thread is available from mdb_last_error().
+ *
+ * Each entry point names the reference interface it replaces
+ * (file:line in the MD_Simulation_CUDA source tree).
+ *
+ * Ownership: the library owns all device memory of a handle. Frames cross the
+ * boundary as caller-owned host buffers in the 64-byte Particle layout of
+ * include/md_particle.hpp:31-38 and are copied in and out.
+ * Threading: a handle may be used by one host thread at a time.
+ */
+#ifndef MDB200_H
+#define MDB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MDB_OK 0
+#define MDB_ERR_CONFIG 1    /* invalid configuration value / unknown key   */
+#define MDB_ERR_ARG 2       /* invalid argument (null, size, range)        */
+#define MDB_ERR_CAPACITY 3  /* a buffer or frame exceeds a stated capacity */
+#define MDB_ERR_NONFINITE 4 /* NaN/Inf detected in the state               */
+#define MDB_ERR_BOX 5       /* invalid box (area <= 0, non-finite)         */
+#define MDB_ERR_CUDA 6      /* CUDA runtime error                          */
+#define MDB_ERR_IO 7        /* file I/O, format or CRC error               */
+#define MDB_ERR_STATE 8     /* call not valid in the current state         */
+#define MDB_ERR_NODEVICE 9  /* no CUDA device available                    */
+
+/* ---- frame layout -------------------------------------------------------
+ * Particle (include/md_particle.hpp:31-38): sizeof 64, align 16,
+ * offsets pos 0 / vel 16 / acc 32 / type 48 / theta 56. acc holds F/m.    */
+typedef struct mdb_double2 {
+  double x, y;
+} mdb_double2_t;
+
+typedef struct mdb_particle {
+  mdb_double2_t pos;
+  mdb_double2_t vel;
+  mdb_double2_t acc;
+  int32_t type;
+  int32_t _pad; /* implicit padding of the reference struct */
+  double theta;
+} mdb_particle_t;
+
+/* ---- configuration ------------------------------------------------------
+ * Field-for-field MDConfig (include/md_config.hpp:14-75); JSON keys are the
+ * field names (src/md_config.cpp:43-130). Strings are NUL-terminated.     */
+typedef struct mdb_config {
+  int32_t n_particles_global;
+  int32_t n_particles_type0;
+  double box_w_global;
+  double box_h_global;
+  double T_init;
+  double T_target;
+  double SIGMA_AA, SIGMA_BB, SIGMA_AB;
+  double EPSILON_AA, EPSILON_BB, EPSILON_AB;
+  double MASS_A, MASS_B;
+  double devide_p;
+  double dt;
+  double Q;
+  double save_dt_interval;
+  double cutoff;
+  char run_name[256];
+  char load_name[256];
+  int32_t THREADS_PER_BLOCK;
+  int32_t rank_size;
+  double mu, v0, D_r, D_theta;
+  double barostat_mass;
+  double k_piston;
+  double barostat_area_rate_init;
+  double barostat_height_min_ratio;
+  double barostat_height_max_ratio;
+  char pressure_target_mode[64];
+  double P_target;
+  int32_t pressure_target_auto_steps;
+  int32_t pressure_eval_interval_steps;
+  int32_t pressure_window_samples;
+  double pressure_tolerance_rel;
+  int32_t pressure_stable_required_windows;
+  int32_t nph_warmup_min_steps;
+  int32_t nph_warmup_max_steps;
+  int32_t nph_steps;
+  int32_t rank_idx;
+  int32_t n_local;
+  int32_t n_halo_left;
+  int32_t n_halo_right;
+  int32_t n_cap;
+  int32_t halo_left_cap;
+  int32_t halo_right_cap;
+  int32_t left_rank;
+  int32_t right_rank;
+  double x_min;
+  double x_max;
+} mdb_config_t;
+
+/* Engine options with no counterpart in MDConfig (B200 engine knobs). */
+typedef struct mdb_options {
+  int32_t device;     /* CUDA device ordinal (default 0)                    */
+  double skin;        /* cell-list skin in sigma units (default 0.3)        */
+  int32_t use_graphs; /* 1: replay captured CUDA graphs for step chunks     */
+  int32_t reserved[13];
+} mdb_options_t;
+
+/* MDConfig{} value-initialised defaults (include/md_config.hpp:14-75). */
+int mdb_config_default(mdb_config_t* out);
+/* MDConfigManager::config_from_json / deserialize (src/md_config.cpp:43-130,
+ * 289-325): keys absent from the JSON object keep the struct defaults. */
+int mdb_config_from_json(const char* json_text, mdb_config_t* out);
+int mdb_config_from_json_file(const char* path, mdb_config_t* out);
+/* MDConfigManager::serialize / config_to_json (src/md_config.cpp:132-195,
+ * 304-319). indent < 0 gives the compact form of serialize(). `needed`
+ * (optional) receives the length excluding the NUL. */
+int mdb_config_to_json(const mdb_config_t* cfg, int32_t indent, char* buf, size_t cap,
+                       size_t* needed);
+/* MDConfigManager::apply_override (src/md_config.cpp:327-452): MDB_OK on
+ * success, MDB_ERR_CONFIG for an unknown key or a value that does not parse. */
+int mdb_config_apply_override(mdb_config_t* cfg, const char* key, const char* value);
+/* MDConfigManager::parse_override_argument (src/md_config.cpp:465-495):
+ * strips "--" then "D", splits on '='. MDB_ERR_ARG when it is not an override. */
+int mdb_parse_override_argument(const char* arg, char* key, size_t key_cap, char* value,
+                                size_t value_cap);
+void mdb_options_default(mdb_options_t* out);
+
+/* ---- PFRAME v2 files (include/md_common.hpp:17-31, src/md_common.cpp:110-320)
+ * 16-byte FileHeader {"PFRAME", version 2, 0}; per frame a packed 36-byte
+ * FrameHeader {frame_index, n, raw bytes, compressed bytes, crc32} and a zlib
+ * (level 9) payload of Particle[n].                                          */
+/* FileWriter(path, append) + write_frame: append != 0 opens an existing file
+ * (validating its header) and appends; otherwise the file is created. */
+int mdb_pframe_write(const char* path, int32_t append, const mdb_particle_t* frame, int64_t n,
+                     uint64_t frame_index);
+/* FileReader + next_frame scan used by MDSimulation(cfg, comm, file, step)
+ * (src/md_env.cu:81-164): finds the first frame whose index equals
+ * frame_index. n_out receives the frame size; when cap < n only n_out is set
+ * and MDB_ERR_CAPACITY is returned. */
+int mdb_pframe_read(const char* path, uint64_t frame_index, mdb_particle_t* out, int64_t cap,
+                    int64_t* n_out);
+/* Number of complete frames and the index of the last one. */
+int mdb_pframe_count(const char* path, int64_t* n_frames, uint64_t* last_index);
+
+/* ---- single-system simulation (class MDSimulation, include/md_env.hpp:51-263)
+ */
+typedef struct mdb_sim mdb_sim_t;
+
+/* MDSimulation(MDConfigManager, MPI_Comm) (src/md_env.cu:21-79) when frame is
+ * NULL: the reference-style lattice initialisation (src/md_env.cu:1276-1445).
+ * With a frame: the frame is loaded as-is (the path the ctor-from-file takes,
+ * src/md_env.cu:81-164). Forces are computed before returning, as the
+ * reference constructors do. n must equal cfg->n_particles_global when frame is
+ * NULL. */
+int mdb_sim_create(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
+                   const mdb_options_t* opt, mdb_sim_t** out);
+/* MDSimulation(cfg, comm, filename, step) (src/md_env.cu:81-164). */
+int mdb_sim_create_from_pframe(const mdb_config_t* cfg, const char* path, uint64_t step,
+                               const mdb_options_t* opt, mdb_sim_t** out);
+int mdb_sim_destroy(mdb_sim_t* sim);
+
+/* step_single_NVE (src/md_env.cu:1576-1637), repeated nsteps times. */
+int mdb_sim_step_nve(mdb_sim_t* sim, int64_t nsteps);
+/* step_single_nose_hoover(do_middle_wrap) (src/md_env.cu:1639-1728).
+ * do_middle_wrap (LG slab reflection) is not part of this library: a
+ * non-zero value returns MDB_ERR_ARG. */
+int mdb_sim_step_nose_hoover(mdb_sim_t* sim, int64_t nsteps, int32_t do_middle_wrap);
+/* step_single_NPH(P_ext) (src/md_env.cu:1795-1918). */
+int mdb_sim_step_nph(mdb_sim_t* sim, double p_ext, int64_t nsteps);
+/* step_single_NPH_piston(P_ext) (src/md_env.cu:1920-2023). */
+int mdb_sim_step_nph_piston(mdb_sim_t* sim, double p_ext, int64_t nsteps);
+
+/* cal_total_K (src/md_env.cu:2141-2146). */
+int mdb_sim_total_K(mdb_sim_t* sim, double* out);
+/* cal_total_U (src/md_env.cu:2347-2360), including wall energy in piston mode. */
+int mdb_sim_total_U(mdb_sim_t* sim, double* out);
+/* cal_instant_pressure (src/md_env.cu:2254-2266). */
+int mdb_sim_instant_pressure(mdb_sim_t* sim, double* out);
+
+typedef struct mdb_observables {
+  double t;                       /* MDSimulation::t                        */
+  double Lx, Ly;                  /* get_Lx / get_Ly                        */
+  double xi;                      /* Nose-Hoover xi                         */
+  double last_instant_pressure;   /* get_last_instant_pressure              */
+  double nph_area_momentum;       /* p_A                                    */
+  double nph_area_rate;           /* get_nph_area_rate                      */
+  double nph_piston_velocity;     /* get_nph_piston_velocity                */
+  double nph_piston_force;        /* get_nph_piston_force                   */
+  int64_t n;                      /* particles                              */
+  int64_t steps;                  /* steps taken since creation             */
+  int64_t rebuilds;               /* cell-list rebuilds since creation      */
+  int32_t piston_mode_active;
+  int32_t nonfinite;              /* 1 when NaN/Inf was seen in the state   */
+} mdb_observables_t;
+int mdb_sim_observables(mdb_sim_t* sim, mdb_observables_t* out);
+
+/* sample_collect + get_host_particles (src/md_env.cu:2502-2514): the frame in
+ * the caller's original particle order. n must equal the particle count. */
+int mdb_sim_get_frame(mdb_sim_t* sim, mdb_particle_t* out, int64_t n);
+/* Replace the state with a frame and recompute forces (ctor semantics). */
+int mdb_sim_set_frame(mdb_sim_t* sim, const mdb_particle_t* frame, int64_t n);
+/* save_env (src/md_env.cu:4106-4124): appends the current frame to a PFRAME
+ * file (created when absent). */
+int mdb_sim_save_pframe(mdb_sim_t* sim, const char* path, uint64_t frame_index);
+int mdb_sim_get_config(mdb_sim_t* sim, mdb_config_t* out);
+/* The cudaStream_t (as void*) all work of this handle is issued on. */
+int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream);
+/* Block until all issued work of the handle has finished. */
+int mdb_sim_synchronize(mdb_sim_t* sim);
+
+/* ---- FIRE minimiser (class EnergyMinimizer, include/md_energy_minimizer.hpp)
+ */
+typedef struct mdb_fire_params { /* FireParams (md_energy_minimizer.hpp:11-25) */
+  double dt_init, dt_max, alpha0, f_inc, f_dec;
+  int32_t N_min;
+  int32_t _pad;
+} mdb_fire_params_t;
+/* FireParams::from_config: dt_init = dt, dt_max = 5 dt, alpha0 0.1,
+ * f_inc 1.1, f_dec 0.5, N_min 5. */
+int mdb_fire_params_from_config(const mdb_config_t* cfg, mdb_fire_params_t* out);
+
+typedef struct mdb_minimize_result { /* MinimizeResult (.hpp:27-35) */
+  int32_t steps;
+  int32_t converged;
+  double max_force;        /* max |a| at the last evaluated iteration */
+  double potential_energy; /* U of the final frame                    */
+  int64_t n_energy_samples;
+  int32_t nonfinite;
+  int32_t _pad;
+} mdb_minimize_result_t;
+
+/* EnergyMinimizer::minimize_frame (src/md_energy_minimizer.cu:122-272) for one
+ * frame. energy_steps / energy_trace receive up to trace_cap samples (step 0,
+ * every 1000 iterations, and the final one). */
+int mdb_fire_minimize(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
+                      double force_tol, int32_t max_steps, const mdb_fire_params_t* params,
+                      const mdb_options_t* opt, mdb_particle_t* frame_out,
+                      mdb_minimize_result_t* result, int32_t* energy_steps,
+                      double* energy_trace, int64_t trace_cap);
+
+/* ---- batched independent systems -------------------------------------------
+ * Many independent systems of uneven N advanced together: one launch per
+ * phase covers every system (per-system cell grids, reductions and scalar
+ * state), so small systems do not leave the GPU idle. The reference runs each
+ * system as a separate job (scripts/submit_batches_*.sh); the per-system
+ * semantics are those of EnergyMinimizer::minimize_frame and the MDSimulation
+ * step functions above. */
+typedef struct mdb_batch mdb_batch_t;
+
+#define MDB_JOB_FIRE 0
+#define MDB_JOB_NVE 1
+#define MDB_JOB_NVT 2 /* Nose-Hoover */
+
+int mdb_batch_create(const mdb_options_t* opt, mdb_batch_t** out);
+int mdb_batch_destroy(mdb_batch_t* b);
+/* Add a FIRE quench (minimize_frame semantics). Returns its id in sys_id. */
+int mdb_batch_add_fire(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
+                       int64_t n, double force_tol, int32_t max_steps,
+                       const mdb_fire_params_t* params, int32_t* sys_id);
+/* Add an MD segment of nsteps steps (MDB_JOB_NVE or MDB_JOB_NVT). */
+int mdb_batch_add_md(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
+                     int64_t n, int32_t kind, int64_t nsteps, int32_t* sys_id);
+/* Advance every unfinished system by up to `iterations` iterations (FIRE
+ * iterations or MD steps); iterations < 0 runs until all are finished. */
+int mdb_batch_run(mdb_batch_t* b, int64_t iterations);
+/* Number of systems and how many are finished. */
+int mdb_batch_progress(mdb_batch_t* b, int32_t* n_systems, int32_t* n_done);
+int mdb_batch_system_info(mdb_batch_t* b, int32_t sys_id, int64_t* n, int32_t* done,
+                          int64_t* steps);
+int mdb_batch_get_frame(mdb_batch_t* b, int32_t sys_id, mdb_particle_t* out, int64_t n);
+int mdb_batch_get_fire_result(mdb_batch_t* b, int32_t sys_id, mdb_minimize_result_t* result,
+                              int32_t* energy_steps, double* energy_trace, int64_t trace_cap);
+int mdb_batch_cuda_stream(mdb_batch_t* b, void** stream);
+
+/* ---- single-call kernels (building blocks, used by tests) ------------------
+ */
+/* li_force_kernel (src/md_cuda_common.cu:151-264) + cal_local_U_kernel
+ * (:703-825) + the pair part of cal_local_pressure_scalar_kernel (:591-701)
+ * for one frame: acc_out (2n doubles, F/m in the frame's order), U (shifted
+ * pair energy) and W = sum_i 1/2 sum_j r.F. periodic_y selects the y image
+ * convention (0 for the piston walls' LJ part). */
+int mdb_compute_forces(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
+                       double Lx, double Ly, int32_t periodic_y, const mdb_options_t* opt,
+                       double* acc_out, double* U_out, double* W_out);
+/* The cell binning of the force path: cell = cy*ncx + cx with
+ * ncx = max(1, floor(Lx/cell_min)), cx = clamp(trunc(x*(ncx/Lx)), 0, ncx-1)
+ * (NaN bins to 0), and perm = the stable sort of particle indices by cell.
+ * pos is 2n doubles (x0,y0,x1,y1,...). cell_out and perm_out hold n ints. */
+int mdb_cell_build(const double* pos, int64_t n, double Lx, double Ly, double cell_min,
+                   int32_t device, int32_t* cell_out, int32_t* perm_out, int32_t* ncx_out,
+                   int32_t* ncy_out);
+
+/* ---- misc --------------------------------------------------------------- */
+/* Copies the last error message of the calling thread (NUL-terminated). */
+int mdb_last_error(char* buf, size_t cap);
+const char* mdb_version(void);
+/* Number of kernel launches this library issued so far (all handles). */
+int64_t mdb_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDB200_H */

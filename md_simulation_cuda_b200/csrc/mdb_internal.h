@@ -1,0 +1,132 @@
+// Internal structures shared by the host engine and the sm_100a kernels.
+//
+// Data layout in HBM (per batch; a single simulation is a batch of one):
+//   particles of all systems are concatenated; system s owns the slots
+//   [p0_s, p0_s + n_s) for its whole life. Inside that range the particles are
+//   kept sorted by cell (re-sorted at every cell-list rebuild); orig[k] maps a
+//   slot back to the caller's particle index.
+//   SoA, FP64 state: pos/vel/acc double2 (16 B each), type int32, theta f64.
+//   pff  float4 per slot: position as an exact float-float pair (hi, lo) in a
+//        biased binade, hi parts' sign bits carry the type class. This is the
+//        only array the pair loop gathers (16 B per candidate).
+//   sb   float2 per slot: position at the last rebuild (fractional for periodic
+//        axes, absolute for the piston's walled y axis).
+//   cells: per system a grid of up to ccap_x*ccap_y cells; the global
+//        exclusive scan cstart[] of per-cell counts gives each cell's slot
+//        range directly because systems are laid out in order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mdb {
+
+constexpr int kThreads = 256;  // particle kernels: one particle per thread
+constexpr int kNP = 6;         // reduction slots per block
+constexpr int kScanItems = 4;  // cells per thread in the scan kernels
+constexpr int kScanBlock = 512;
+constexpr int kScanTile = kScanItems * kScanBlock;
+
+// Force-phase variants.
+enum FMode : int32_t {
+  FM_INIT = 0,    // acc = F/m (constructor / set_frame / piston entry)
+  FM_NVE = 1,     // + second velocity-Verlet half kick
+  FM_NH = 2,      // + Nose-Hoover second half kick, K reduction
+  FM_NPH = 3,     // + virial, kinetic before/after kick, barostat half step
+  FM_PISTON = 4,  // + soft walls, piston half step
+  FM_FIRE = 5,    // + full kick, FIRE statistics and control
+  FM_OBS = 6,     // no state change: U, virial, kinetic, wall terms
+};
+
+// Drift-phase variants.
+enum DMode : int32_t { DM_NVE = 0, DM_NH = 1, DM_NPH = 2, DM_PISTON = 3, DM_FIRE = 4 };
+
+// Job kinds of a batch system.
+enum Kind : int32_t { K_FIRE = 0, K_NVE = 1, K_NVT = 2 };
+
+struct SysParams {
+  int64_t p0;     // first slot
+  int64_t c0;     // first cell
+  int32_t n;      // particles
+  int32_t b0;     // first block of the block table
+  int32_t nb;     // blocks
+  int32_t ccap_x, ccap_y;
+  int32_t kind;
+  double sig[3], eps[3], Vc[3];  // AA, BB, AB
+  double massA, massB, cutoff, rc_max, r_cell, skin;
+  double dt, Q, T0, g_dof, W, k_piston, hmin, hmax, Lx0, Ly0, rate_init;
+  double offx, offy;             // binade offsets of the float-float split
+  float fsig2[3], feps24[3], feps4[3], frc2[3];
+  // FIRE
+  double f_dt_max, f_alpha0, f_inc, f_dec, f_tol;
+  int32_t f_Nmin, f_max_steps;
+  int64_t target_steps;  // MD segment length (batches)
+};
+
+struct SysState {
+  double Lx, Ly;
+  double xi, K;                       // Nose-Hoover
+  double pA, aspect, P_cur, last_P;   // NPH
+  double fl, ce;                      // Ly clamp bounds
+  double vp, Fp, wallU;               // piston
+  double U, Wv, kin, kin2;            // last observable reductions
+  double p_ext;                       // external pressure of the running call
+  double inv_wx, inv_wy, Lx_b, Ly_b;  // cell grid at the last rebuild
+  int32_t ncx, ncy, allpairs, periodic_y;
+  int32_t clamped, nph_init, piston_active, piston_init;
+  uint32_t dmax_x, dmax_y, jump;      // float bits (non-negative)
+  int32_t need_rebuild;
+  int32_t nonfinite;
+  int32_t err;
+  uint32_t counter;
+  int32_t done;                        // finished job (batches)
+  int64_t steps, rebuilds;
+  // FIRE
+  double f_dt, f_alpha, f_maxf, f_power;
+  int32_t f_streak, f_conv, f_zero_v, f_step;
+  int32_t f_conv_step;
+  int32_t pad_;
+};
+
+struct BatchGlobal {
+  int32_t any_rebuild;
+  uint32_t sys_counter;
+  int32_t nsys;
+  int32_t all_done;
+};
+
+// Kernel argument block (passed by value).
+struct Dev {
+  const int32_t* sys_of_block;
+  const int32_t* sysid;  // per slot
+  const SysParams* sp;
+  SysState* st;
+  BatchGlobal* bg;
+  double2 *pos, *vel, *acc;
+  int32_t* type;
+  double* theta;
+  int32_t* orig;
+  double2 *pos2, *vel2, *acc2;
+  int32_t* type2;
+  double* theta2;
+  int32_t* orig2;
+  float4* pff;
+  float2* sb;
+  int32_t* cell_of;
+  int32_t* key;
+  int32_t* perm;
+  int32_t* ccount;
+  int32_t* ccursor;
+  int32_t* cstart;    // ncells + 1
+  int32_t* scan_part; // per scan tile
+  double* part;       // nblocks * kNP
+  int32_t nsys;
+  int32_t nblocks;
+  int64_t ntot;
+  int64_t ncells;
+  cudaGraphConditionalHandle cond;
+  int32_t use_cond;
+  int32_t rb_grid;    // grid of the grid-stride rebuild kernels
+};
+
+}  // namespace mdb
