@@ -1,0 +1,478 @@
+"""md_simulation_cuda_b200 — B200-native MD stepping path of MD_Simulation_CUDA.
+
+Python mirror of the reference's C++ surface for the hot path, over the C ABI of
+``libmdb200.so`` (include/mdb200.h):
+
+* ``MDConfig`` / ``MDConfigManager``  — include/md_config.hpp:14-111
+* ``MDSimulation``                    — include/md_env.hpp:51-263 (hot path)
+* ``EnergyMinimizer``, ``FireParams``, ``MinimizeResult``
+                                      — include/md_energy_minimizer.hpp:11-97
+* ``FileWriter`` / ``FileReader``     — include/md_common.hpp:88-122 (PFRAME v2)
+* ``Batch``                           — many independent systems in one launch
+
+Frames are numpy arrays of ``PARTICLE_DTYPE`` (the 64-byte Particle of
+include/md_particle.hpp:31-38). The MPI communicator arguments of the reference
+are accepted and ignored: one process drives one GPU and resolves every
+periodic image itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from ._lib import (MDB_ERR_ARG, MDBConfigC, MDBError, MDBFireParams, MDBMinimizeResult,
+                   MDBObservables, PARTICLE_DTYPE, check, frame_ptr, lib, options)
+
+__all__ = [
+    "PARTICLE_DTYPE", "MDBError", "MDConfig", "MDConfigManager", "MDSimulation",
+    "EnergyMinimizer", "FireParams", "MinimizeResult", "FileWriter", "FileReader", "Batch",
+    "make_frame", "compute_forces", "cell_build", "kernel_launches",
+]
+
+MDConfig = MDBConfigC  # field-for-field MDConfig
+
+
+def make_frame(n: int) -> np.ndarray:
+    """A zeroed frame of n particles."""
+    return np.zeros(n, dtype=PARTICLE_DTYPE)
+
+
+def _as_frame(frame) -> np.ndarray:
+    f = np.ascontiguousarray(frame)
+    if f.dtype != PARTICLE_DTYPE:
+        raise TypeError("frame must have PARTICLE_DTYPE")
+    return f
+
+
+class MDConfigManager:
+    """MDConfigManager (include/md_config.hpp:82-111, src/md_config.cpp)."""
+
+    def __init__(self, config: Optional[MDBConfigC] = None):
+        if config is None:
+            config = MDBConfigC()
+            check(lib().mdb_config_default(C.byref(config)))
+        self.config = config
+
+    @staticmethod
+    def config_from_json(filepath: str) -> "MDConfigManager":
+        cfg = MDBConfigC()
+        if not os.path.exists(filepath):
+            raise RuntimeError("Failed to open config file: " + str(filepath))
+        check(lib().mdb_config_from_json_file(os.fsencode(filepath), C.byref(cfg)))
+        return MDConfigManager(cfg)
+
+    def _dump(self, indent: int) -> str:
+        need = C.c_size_t(0)
+        check(lib().mdb_config_to_json(C.byref(self.config), indent, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(need.value + 1)
+        check(lib().mdb_config_to_json(C.byref(self.config), indent, buf, len(buf), None))
+        return buf.value.decode()
+
+    def config_to_json(self, filepath: str) -> None:
+        try:
+            with open(filepath, "w") as f:
+                f.write(self._dump(4) + "\n")
+        except OSError as e:
+            raise RuntimeError("Failed to open config file for writing: " + str(filepath)) from e
+
+    def serialize(self) -> str:
+        return self._dump(-1)
+
+    def deserialize(self, data: str) -> None:
+        # load_from_json_object starts from struct defaults, like the reference
+        cfg = MDBConfigC()
+        check(lib().mdb_config_from_json(data.encode(), C.byref(cfg)))
+        self.config = cfg
+
+    def apply_override(self, key: str, value: str) -> bool:
+        rc = lib().mdb_config_apply_override(C.byref(self.config), key.encode(), value.encode())
+        return rc == 0
+
+    def apply_overrides(self, overrides: Sequence) -> None:
+        for item in overrides:
+            key, value = (item.key, item.value) if hasattr(item, "key") else item
+            if not self.apply_override(key, value):
+                raise RuntimeError(f"Invalid override '{key}={value}'")
+
+    @staticmethod
+    def parse_override_argument(argument: str):
+        """(key, value) or None, like the reference's bool + out parameters."""
+        k = C.create_string_buffer(1024)
+        v = C.create_string_buffer(4096)
+        rc = lib().mdb_parse_override_argument(argument.encode(), k, len(k), v, len(v))
+        if rc != 0:
+            return None
+        return k.value.decode(), v.value.decode()
+
+    def copy(self) -> "MDConfigManager":
+        c = MDBConfigC()
+        C.memmove(C.byref(c), C.byref(self.config), C.sizeof(MDBConfigC))
+        return MDConfigManager(c)
+
+
+def _config_of(cfg) -> MDBConfigC:
+    if isinstance(cfg, MDConfigManager):
+        return cfg.config
+    if isinstance(cfg, MDBConfigC):
+        return cfg
+    if isinstance(cfg, dict):
+        m = MDConfigManager()
+        for k, v in cfg.items():
+            if isinstance(v, str):
+                setattr(m.config, k, v.encode())
+            else:
+                setattr(m.config, k, v)
+        return m.config
+    raise TypeError("expected MDConfigManager, MDConfig or dict")
+
+
+class MDSimulation:
+    """The stepping part of class MDSimulation (include/md_env.hpp:51-263).
+
+    MDSimulation(cfg, comm)                -> lattice initialisation
+    MDSimulation(cfg, comm, filename, step) -> frame `step` of a PFRAME file
+    MDSimulation(cfg, frame=array)          -> an in-memory frame
+    """
+
+    def __init__(self, config_manager, comm=None, filename: Optional[str] = None,
+                 step: Optional[int] = None, *, frame=None, device: int = 0,
+                 skin: Optional[float] = None, use_graphs: bool = True):
+        self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
+            else MDConfigManager(_config_of(config_manager))
+        self._h = C.c_void_p()
+        opt = options(device, skin, use_graphs)
+        cfg = self.cfg_manager.config
+        if filename is not None:
+            check(lib().mdb_sim_create_from_pframe(C.byref(cfg), os.fsencode(filename),
+                                                   int(step or 0), C.byref(opt),
+                                                   C.byref(self._h)))
+        elif frame is not None:
+            f = _as_frame(frame)
+            check(lib().mdb_sim_create(C.byref(cfg), frame_ptr(f), len(f), C.byref(opt),
+                                       C.byref(self._h)))
+        else:
+            check(lib().mdb_sim_create(C.byref(cfg), None, 0, C.byref(opt), C.byref(self._h)))
+        self._h_particles = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mdb_sim_destroy(h)
+            except Exception:
+                pass
+            self._h = C.c_void_p()
+
+    def close(self):
+        self.__del__()
+
+    # ---- steps --------------------------------------------------------
+    def step_single_NVE(self, nsteps: int = 1) -> None:
+        check(lib().mdb_sim_step_nve(self._h, nsteps))
+
+    step_single = step_single_NVE  # README.md:27 name
+
+    def step_single_nose_hoover(self, do_middle_wrap: bool = False, nsteps: int = 1) -> None:
+        check(lib().mdb_sim_step_nose_hoover(self._h, nsteps, 1 if do_middle_wrap else 0))
+
+    def step_single_NPH(self, pressure_ext: float, nsteps: int = 1) -> None:
+        check(lib().mdb_sim_step_nph(self._h, float(pressure_ext), nsteps))
+
+    def step_single_NPH_piston(self, pressure_ext: float, nsteps: int = 1) -> None:
+        check(lib().mdb_sim_step_nph_piston(self._h, float(pressure_ext), nsteps))
+
+    # ---- observables --------------------------------------------------
+    def _scalar(self, fn) -> float:
+        out = C.c_double()
+        check(fn(self._h, C.byref(out)))
+        return out.value
+
+    def cal_total_K(self) -> float:
+        return self._scalar(lib().mdb_sim_total_K)
+
+    def cal_total_U(self) -> float:
+        return self._scalar(lib().mdb_sim_total_U)
+
+    def cal_instant_pressure(self) -> float:
+        return self._scalar(lib().mdb_sim_instant_pressure)
+
+    def observables(self) -> MDBObservables:
+        o = MDBObservables()
+        check(lib().mdb_sim_observables(self._h, C.byref(o)))
+        return o
+
+    @property
+    def t(self) -> float:
+        return self.observables().t
+
+    def get_Lx(self) -> float:
+        return self.observables().Lx
+
+    def get_Ly(self) -> float:
+        return self.observables().Ly
+
+    def get_last_instant_pressure(self) -> float:
+        return self.observables().last_instant_pressure
+
+    def get_nph_area_rate(self) -> float:
+        return self.observables().nph_area_rate
+
+    def get_nph_piston_velocity(self) -> float:
+        return self.observables().nph_piston_velocity
+
+    def get_nph_piston_force(self) -> float:
+        return self.observables().nph_piston_force
+
+    @property
+    def xi(self) -> float:
+        return self.observables().xi
+
+    # ---- frames -------------------------------------------------------
+    def n_particles(self) -> int:
+        return int(self.observables().n)
+
+    def sample_collect(self) -> None:
+        n = self.n_particles()
+        f = make_frame(n)
+        check(lib().mdb_sim_get_frame(self._h, frame_ptr(f), n))
+        self._h_particles = f
+
+    def get_host_particles(self) -> np.ndarray:
+        if self._h_particles is None:
+            self.sample_collect()
+        return self._h_particles.copy()
+
+    def set_frame(self, frame) -> None:
+        f = _as_frame(frame)
+        check(lib().mdb_sim_set_frame(self._h, frame_ptr(f), len(f)))
+
+    def save_env(self, filename: str, step: int) -> None:
+        check(lib().mdb_sim_save_pframe(self._h, os.fsencode(filename), int(step)))
+
+    def synchronize(self) -> None:
+        check(lib().mdb_sim_synchronize(self._h))
+
+    def cuda_stream(self) -> int:
+        p = C.c_void_p()
+        check(lib().mdb_sim_cuda_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+
+@dataclass
+class FireParams:
+    """FireParams (include/md_energy_minimizer.hpp:11-25)."""
+    dt_init: float = 0.0
+    dt_max: float = 0.0
+    alpha0: float = 0.1
+    f_inc: float = 1.1
+    f_dec: float = 0.5
+    N_min: int = 5
+
+    @staticmethod
+    def from_config(cfg) -> "FireParams":
+        c = _config_of(cfg)
+        return FireParams(dt_init=c.dt, dt_max=5.0 * c.dt)
+
+    def _c(self) -> MDBFireParams:
+        return MDBFireParams(self.dt_init, self.dt_max, self.alpha0, self.f_inc, self.f_dec,
+                             int(self.N_min), 0)
+
+
+@dataclass
+class MinimizeResult:
+    """MinimizeResult (include/md_energy_minimizer.hpp:27-35)."""
+    frame: np.ndarray = field(default_factory=lambda: make_frame(0))
+    energy_steps: List[int] = field(default_factory=list)
+    energy_trace: List[float] = field(default_factory=list)
+    steps: int = 0
+    converged: bool = False
+    max_force: float = 0.0
+    potential_energy: float = 0.0
+    nonfinite: bool = False
+
+
+class EnergyMinimizer:
+    """EnergyMinimizer (include/md_energy_minimizer.hpp:37-97)."""
+
+    def __init__(self, config_manager, comm=None, *, device: int = 0,
+                 skin: Optional[float] = None, use_graphs: bool = True):
+        self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
+            else MDConfigManager(_config_of(config_manager))
+        # allocate_buffers (src/md_energy_minimizer.cu:92-100)
+        if self.cfg_manager.config.n_cap <= 0:
+            raise RuntimeError("EnergyMinimizer: n_cap must be positive.")
+        self._opt = options(device, skin, use_graphs)
+
+    def minimize_frame(self, frame, force_tol: float, max_steps: int,
+                       params: FireParams) -> MinimizeResult:
+        f = _as_frame(frame)
+        if max_steps <= 0:
+            raise RuntimeError("EnergyMinimizer: max_steps must be positive.")
+        if len(f) > self.cfg_manager.config.n_cap:
+            raise RuntimeError("EnergyMinimizer: input frame exceeds buffer capacity.")
+        out = make_frame(len(f))
+        res = MDBMinimizeResult()
+        cap = max_steps // 1000 + 4
+        es = np.zeros(cap, dtype=np.int32)
+        et = np.zeros(cap, dtype=np.float64)
+        p = params._c()
+        check(lib().mdb_fire_minimize(
+            C.byref(self.cfg_manager.config), frame_ptr(f), len(f), float(force_tol),
+            int(max_steps), C.byref(p), C.byref(self._opt), frame_ptr(out), C.byref(res),
+            es.ctypes.data_as(C.POINTER(C.c_int32)), et.ctypes.data_as(C.POINTER(C.c_double)),
+            cap))
+        k = min(res.n_energy_samples, cap)
+        return MinimizeResult(frame=out, energy_steps=es[:k].tolist(),
+                              energy_trace=et[:k].tolist(), steps=res.steps,
+                              converged=bool(res.converged), max_force=res.max_force,
+                              potential_energy=res.potential_energy,
+                              nonfinite=bool(res.nonfinite))
+
+
+class FileWriter:
+    """FileWriter (include/md_common.hpp:88-99): PFRAME v2 frames."""
+
+    def __init__(self, path: str, append: bool):
+        self.path = path
+        if append:
+            n = C.c_int64()
+            last = C.c_uint64()
+            rc = lib().mdb_pframe_count(os.fsencode(path), C.byref(n), C.byref(last))
+            if rc != 0 and not os.path.exists(path):
+                raise RuntimeError("Failed to open file for append: " + path)
+            self._fresh = False
+        else:
+            self._fresh = True
+
+    def write_frame(self, data, frame_index: int) -> None:
+        f = _as_frame(data)
+        check(lib().mdb_pframe_write(os.fsencode(self.path), 0 if self._fresh else 1,
+                                     frame_ptr(f), len(f), int(frame_index)))
+        self._fresh = False
+
+
+class FileReader:
+    """FileReader (include/md_common.hpp:101-122)."""
+
+    def __init__(self, path: str):
+        self.path = path
+        n = C.c_int64()
+        last = C.c_uint64()
+        check(lib().mdb_pframe_count(os.fsencode(path), C.byref(n), C.byref(last)))
+        self.n_frames = n.value
+
+    def read(self, frame_index: int) -> np.ndarray:
+        n = C.c_int64()
+        rc = lib().mdb_pframe_read(os.fsencode(self.path), int(frame_index), None, 0, C.byref(n))
+        if rc not in (0, 3):
+            check(rc)
+        f = make_frame(n.value)
+        check(lib().mdb_pframe_read(os.fsencode(self.path), int(frame_index), frame_ptr(f),
+                                    n.value, C.byref(n)))
+        return f
+
+
+class Batch:
+    """Many independent FIRE quenches advanced together on one GPU."""
+
+    def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True):
+        self._h = C.c_void_p()
+        self._opt = options(device, skin, use_graphs)
+        check(lib().mdb_batch_create(C.byref(self._opt), C.byref(self._h)))
+        self._sizes = []
+        self._caps = []
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mdb_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = C.c_void_p()
+
+    def add_fire(self, config, frame, force_tol: float, max_steps: int,
+                 params: FireParams) -> int:
+        f = _as_frame(frame)
+        sid = C.c_int32()
+        p = params._c()
+        check(lib().mdb_batch_add_fire(self._h, C.byref(_config_of(config)), frame_ptr(f), len(f),
+                                       float(force_tol), int(max_steps), C.byref(p),
+                                       C.byref(sid)))
+        self._sizes.append(len(f))
+        self._caps.append(max_steps // 1000 + 4)
+        return sid.value
+
+    def run(self, iterations: int = -1) -> None:
+        check(lib().mdb_batch_run(self._h, int(iterations)))
+
+    def progress(self):
+        a = C.c_int32()
+        b = C.c_int32()
+        check(lib().mdb_batch_progress(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def frame(self, sys_id: int) -> np.ndarray:
+        f = make_frame(self._sizes[sys_id])
+        check(lib().mdb_batch_get_frame(self._h, sys_id, frame_ptr(f), len(f)))
+        return f
+
+    def fire_result(self, sys_id: int, with_frame: bool = True) -> MinimizeResult:
+        res = MDBMinimizeResult()
+        cap = self._caps[sys_id]
+        es = np.zeros(cap, dtype=np.int32)
+        et = np.zeros(cap, dtype=np.float64)
+        check(lib().mdb_batch_get_fire_result(self._h, sys_id, C.byref(res),
+                                              es.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              et.ctypes.data_as(C.POINTER(C.c_double)), cap))
+        k = min(res.n_energy_samples, cap)
+        return MinimizeResult(frame=self.frame(sys_id) if with_frame else make_frame(0),
+                              energy_steps=es[:k].tolist(), energy_trace=et[:k].tolist(),
+                              steps=res.steps, converged=bool(res.converged),
+                              max_force=res.max_force, potential_energy=res.potential_energy,
+                              nonfinite=bool(res.nonfinite))
+
+    def cuda_stream(self) -> int:
+        p = C.c_void_p()
+        check(lib().mdb_batch_cuda_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+
+def compute_forces(config, frame, Lx: float, Ly: float, periodic_y: bool = True,
+                   device: int = 0, skin: Optional[float] = None):
+    """One force evaluation: (acc[n,2], U, W)."""
+    f = _as_frame(frame)
+    n = len(f)
+    acc = np.zeros((n, 2))
+    U = C.c_double()
+    W = C.c_double()
+    opt = options(device, skin)
+    check(lib().mdb_compute_forces(C.byref(_config_of(config)), frame_ptr(f), n, float(Lx),
+                                   float(Ly), 1 if periodic_y else 0, C.byref(opt),
+                                   acc.ctypes.data_as(C.POINTER(C.c_double)), C.byref(U),
+                                   C.byref(W)))
+    return acc, U.value, W.value
+
+
+def cell_build(pos, Lx: float, Ly: float, cell_min: float, device: int = 0):
+    """GPU cell binning: (cell ids, stable permutation, ncx, ncy)."""
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 2)
+    n = p.shape[0]
+    cell = np.zeros(n, dtype=np.int32)
+    perm = np.zeros(n, dtype=np.int32)
+    ncx = C.c_int32()
+    ncy = C.c_int32()
+    check(lib().mdb_cell_build(p.ctypes.data_as(C.POINTER(C.c_double)), n, float(Lx), float(Ly),
+                               float(cell_min), device,
+                               cell.ctypes.data_as(C.POINTER(C.c_int32)),
+                               perm.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(ncx),
+                               C.byref(ncy)))
+    return cell, perm, ncx.value, ncy.value
+
+
+def kernel_launches() -> int:
+    return int(lib().mdb_kernel_launches())

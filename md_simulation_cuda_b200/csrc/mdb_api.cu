@@ -1,0 +1,699 @@
+// extern "C" entry points of libmdb200 (declared in include/mdb200.h).
+// The reference-facing semantics (MDSimulation, EnergyMinimizer) live here on
+// top of the engine; each function cites the reference code it replaces.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "mdb200.h"
+#include "mdb_engine.h"
+#include "mdb_util.h"
+
+using mdb::Engine;
+using mdb::SysState;
+using mdb::SystemSpec;
+
+struct mdb_sim {
+  std::unique_ptr<Engine> eng;
+  mdb_config_t cfg;
+  double t = 0.0;
+  bool piston_active = false;  // piston_mode_active (md_env.hpp:218)
+  bool k_valid = false;        // S.K holds K of the current velocities
+  bool p_valid = false;        // S.P_cur holds the current scalar pressure
+  bool nph_init = false;       // nph_state_initialized
+  bool vp_init = false;        // nph_piston_velocity_initialized
+  int periodic_y = 1;          // y convention of the cell binning
+};
+
+namespace {
+
+#define MDB_TRY(expr)            \
+  do {                           \
+    int rc_ = (expr);            \
+    if (rc_ != MDB_OK) return rc_; \
+  } while (0)
+
+mdb_options_t opts_or_default(const mdb_options_t* opt) {
+  mdb_options_t o;
+  mdb_options_default(&o);
+  if (opt) o = *opt;
+  return o;
+}
+
+int check_status(mdb_sim_t* sim) {
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  if (S.err == MDB_ERR_BOX) return mdb::set_error(MDB_ERR_BOX, "invalid box (area <= 0 or non-finite) in a barostat step");
+  if (S.err) return mdb::set_error(S.err, "device error flag set");
+  return MDB_OK;
+}
+
+int sim_make(const mdb_config_t* cfg, std::vector<mdb_particle_t>&& frame,
+             const mdb_options_t* opt, mdb_sim_t** out) {
+  std::unique_ptr<mdb_sim> sim(new (std::nothrow) mdb_sim());
+  if (!sim) return mdb::set_error(MDB_ERR_CAPACITY, "out of host memory");
+  sim->cfg = *cfg;
+  mdb_options_t o = opts_or_default(opt);
+  sim->eng.reset(new Engine(o));
+  SystemSpec spec;
+  spec.cfg = *cfg;
+  spec.frame = std::move(frame);
+  spec.kind = mdb::K_NVE;
+  MDB_TRY(sim->eng->add_system(std::move(spec)));
+  MDB_TRY(sim->eng->build());
+  // the constructors end with cal_forces() (src/md_env.cu:61-79, 147-158)
+  MDB_TRY(sim->eng->force(mdb::FM_INIT, true));
+  MDB_TRY(sim->eng->sync());
+  *out = sim.release();
+  return MDB_OK;
+}
+
+// Leaves the piston's walled y convention (every non-piston step sets
+// piston_mode_active = false, src/md_env.cu:1577, 1640, 1796).
+int leave_piston(mdb_sim_t* sim) {
+  sim->piston_active = false;
+  if (sim->periodic_y != 1) {
+    MDB_TRY(sim->eng->rebuild_now(1));
+    sim->periodic_y = 1;
+  }
+  return MDB_OK;
+}
+
+void advance_time(mdb_sim_t* sim, int64_t n) {
+  for (int64_t k = 0; k < n; ++k) sim->t += sim->cfg.dt;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdb_sim_create(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
+                   const mdb_options_t* opt, mdb_sim_t** out) {
+  if (!cfg || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  *out = nullptr;
+  std::vector<mdb_particle_t> f;
+  if (frame) {
+    if (n <= 0) return mdb::set_error(MDB_ERR_ARG, "frame size must be positive");
+    f.assign(frame, frame + n);
+  } else {
+    MDB_TRY(mdb::reference_initial_frame(*cfg, f));
+    if (n > 0 && n != (int64_t)f.size())
+      return mdb::set_error(MDB_ERR_ARG, "n must equal n_particles_global");
+  }
+  return sim_make(cfg, std::move(f), opt, out);
+}
+
+int mdb_sim_create_from_pframe(const mdb_config_t* cfg, const char* path, uint64_t step,
+                               const mdb_options_t* opt, mdb_sim_t** out) {
+  if (!cfg || !path || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  *out = nullptr;
+  int64_t n = 0;
+  int rc = mdb_pframe_read(path, step, nullptr, 0, &n);
+  if (rc != MDB_OK && rc != MDB_ERR_CAPACITY) return rc;
+  if (n <= 0) return mdb::set_error(MDB_ERR_IO, "frame is empty");
+  std::vector<mdb_particle_t> f((size_t)n);
+  MDB_TRY(mdb_pframe_read(path, step, f.data(), n, &n));
+  return sim_make(cfg, std::move(f), opt, out);
+}
+
+int mdb_sim_destroy(mdb_sim_t* sim) {
+  delete sim;
+  return MDB_OK;
+}
+
+int mdb_sim_step_nve(mdb_sim_t* sim, int64_t nsteps) {
+  if (!sim || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (nsteps == 0) return MDB_OK;
+  MDB_TRY(leave_piston(sim));
+  MDB_TRY(sim->eng->run_md(mdb::DM_NVE, mdb::FM_NVE, true, nsteps));
+  sim->k_valid = false;
+  sim->p_valid = false;
+  advance_time(sim, nsteps);
+  return MDB_OK;
+}
+
+int mdb_sim_step_nose_hoover(mdb_sim_t* sim, int64_t nsteps, int32_t do_middle_wrap) {
+  if (!sim || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (do_middle_wrap)
+    return mdb::set_error(MDB_ERR_ARG, "do_middle_wrap (LG slab reflection) is not provided");
+  if (nsteps == 0) return MDB_OK;
+  MDB_TRY(leave_piston(sim));
+  if (!sim->k_valid) MDB_TRY(sim->eng->reduce_K());
+  MDB_TRY(sim->eng->run_md(mdb::DM_NH, mdb::FM_NH, true, nsteps));
+  sim->k_valid = true;
+  sim->p_valid = false;
+  advance_time(sim, nsteps);
+  return MDB_OK;
+}
+
+int mdb_sim_step_nph(mdb_sim_t* sim, double p_ext, int64_t nsteps) {
+  if (!sim || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (nsteps == 0) return MDB_OK;
+  MDB_TRY(leave_piston(sim));
+  SysState S;
+  if (!sim->nph_init || !sim->p_valid) {
+    if (!sim->p_valid) MDB_TRY(sim->eng->force(mdb::FM_OBS, true));
+    MDB_TRY(sim->eng->get_state(0, &S));
+    if (S.err) return check_status(sim);
+    if (!sim->nph_init) {
+      // init_nph_state_if_needed (src/md_env.cu:1757-1778)
+      if (!(S.Lx > 0.0) || !(S.Ly > 0.0))
+        return mdb::set_error(MDB_ERR_BOX, "invalid initial box for NPH");
+      S.aspect = S.Lx / S.Ly;
+      const double W = sim->cfg.barostat_mass > 1e-12 ? sim->cfg.barostat_mass : 1e-12;
+      S.pA = W * sim->cfg.barostat_area_rate_init;
+      sim->nph_init = true;
+    }
+    if (!sim->p_valid) {
+      const double A = S.Lx * S.Ly;
+      S.P_cur = (A > 0.0) ? (S.kin + S.Wv) / (2.0 * A) : 0.0;
+    }
+    MDB_TRY(sim->eng->put_state(0, S));
+  }
+  MDB_TRY(sim->eng->set_pext(p_ext));
+  MDB_TRY(sim->eng->run_md(mdb::DM_NPH, mdb::FM_NPH, true, nsteps));
+  sim->p_valid = true;
+  sim->k_valid = false;
+  advance_time(sim, nsteps);
+  return MDB_OK;
+}
+
+int mdb_sim_step_nph_piston(mdb_sim_t* sim, double p_ext, int64_t nsteps) {
+  if (!sim || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (nsteps == 0) return MDB_OK;
+  if (!sim->vp_init || !sim->piston_active) {
+    // init_nph_piston_state_if_needed (src/md_env.cu:1780-1793)
+    if (!sim->piston_active) {
+      if (sim->periodic_y != 0) {
+        MDB_TRY(sim->eng->rebuild_now(0));
+        sim->periodic_y = 0;
+      }
+      MDB_TRY(sim->eng->force(mdb::FM_INIT, false));
+    }
+    SysState S;
+    MDB_TRY(sim->eng->get_state(0, &S));
+    if (!sim->vp_init) {
+      S.vp = 0.0;
+      sim->vp_init = true;
+    }
+    if (!sim->piston_active) {
+      S.last_P = (S.Lx > 0.0) ? (S.Fp / S.Lx) : 0.0;
+      sim->piston_active = true;
+    }
+    MDB_TRY(sim->eng->put_state(0, S));
+  }
+  MDB_TRY(sim->eng->set_pext(p_ext));
+  MDB_TRY(sim->eng->run_md(mdb::DM_PISTON, mdb::FM_PISTON, false, nsteps));
+  sim->k_valid = false;
+  sim->p_valid = false;
+  advance_time(sim, nsteps);
+  return MDB_OK;
+}
+
+int mdb_sim_total_K(mdb_sim_t* sim, double* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(sim->eng->reduce_K());
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  sim->k_valid = true;
+  *out = S.K;
+  return check_status(sim);
+}
+
+int mdb_sim_total_U(mdb_sim_t* sim, double* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(sim->eng->force(mdb::FM_OBS, !sim->piston_active));
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  *out = sim->piston_active ? S.U + S.wallU : S.U;
+  return check_status(sim);
+}
+
+int mdb_sim_instant_pressure(mdb_sim_t* sim, double* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(sim->eng->force(mdb::FM_OBS, !sim->piston_active));
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  if (sim->piston_active) {
+    S.Fp = S.kin2;
+    S.last_P = (S.Lx > 0.0) ? (S.Fp / S.Lx) : 0.0;
+  } else {
+    const double A = S.Lx * S.Ly;
+    S.last_P = (A > 0.0) ? (S.kin + S.Wv) / (2.0 * A) : 0.0;
+    S.P_cur = S.last_P;
+    sim->p_valid = true;
+  }
+  MDB_TRY(sim->eng->put_state(0, S));
+  *out = S.last_P;
+  return check_status(sim);
+}
+
+int mdb_sim_observables(mdb_sim_t* sim, mdb_observables_t* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  memset(out, 0, sizeof(*out));
+  out->t = sim->t;
+  out->Lx = S.Lx;
+  out->Ly = S.Ly;
+  out->xi = S.xi;
+  out->last_instant_pressure = S.last_P;
+  out->nph_area_momentum = S.pA;
+  const double W = sim->cfg.barostat_mass > 1e-12 ? sim->cfg.barostat_mass : 1e-12;
+  out->nph_area_rate = S.pA / W;
+  out->nph_piston_velocity = S.vp;
+  out->nph_piston_force = S.Fp;
+  out->n = sim->eng->n(0);
+  out->steps = S.steps;
+  out->rebuilds = S.rebuilds;
+  out->piston_mode_active = sim->piston_active ? 1 : 0;
+  out->nonfinite = S.nonfinite;
+  return check_status(sim);
+}
+
+int mdb_sim_get_frame(mdb_sim_t* sim, mdb_particle_t* out, int64_t n) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  if (n != sim->eng->n(0)) return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the particle count");
+  return sim->eng->get_frame(0, out);
+}
+
+int mdb_sim_set_frame(mdb_sim_t* sim, const mdb_particle_t* frame, int64_t n) {
+  if (!sim || !frame) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  if (n != sim->eng->n(0)) return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the particle count");
+  MDB_TRY(sim->eng->set_frame(0, frame));
+  MDB_TRY(sim->eng->rebuild_now(sim->periodic_y));
+  MDB_TRY(sim->eng->force(mdb::FM_INIT, sim->periodic_y != 0));
+  sim->k_valid = false;
+  sim->p_valid = false;
+  return sim->eng->sync();
+}
+
+int mdb_sim_save_pframe(mdb_sim_t* sim, const char* path, uint64_t frame_index) {
+  if (!sim || !path) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  std::vector<mdb_particle_t> f((size_t)sim->eng->n(0));
+  MDB_TRY(sim->eng->get_frame(0, f.data()));
+  // save_env: open for append, create the file when that fails
+  int rc = mdb_pframe_write(path, 1, f.data(), (int64_t)f.size(), frame_index);
+  if (rc != MDB_OK) rc = mdb_pframe_write(path, 0, f.data(), (int64_t)f.size(), frame_index);
+  return rc;
+}
+
+int mdb_sim_get_config(mdb_sim_t* sim, mdb_config_t* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  *out = sim->cfg;
+  out->box_w_global = S.Lx;
+  out->box_h_global = S.Ly;
+  return MDB_OK;
+}
+
+int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream) {
+  if (!sim || !stream) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  *stream = (void*)sim->eng->stream();
+  return MDB_OK;
+}
+
+int mdb_sim_synchronize(mdb_sim_t* sim) {
+  if (!sim) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(sim->eng->sync());
+  return check_status(sim);
+}
+
+// ------------------------------------------------------------------ FIRE --
+
+int mdb_fire_params_from_config(const mdb_config_t* cfg, mdb_fire_params_t* out) {
+  if (!cfg || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  memset(out, 0, sizeof(*out));
+  out->dt_init = cfg->dt;
+  out->dt_max = 5.0 * cfg->dt;
+  out->alpha0 = 0.1;
+  out->f_inc = 1.1;
+  out->f_dec = 0.5;
+  out->N_min = 5;
+  return MDB_OK;
+}
+
+namespace {
+
+// Energy samples of one FIRE run (MinimizeResult::energy_steps/_trace).
+struct Trace {
+  std::vector<int32_t> steps;
+  std::vector<double> u;
+  void add(int32_t s, double v) {
+    steps.push_back(s);
+    u.push_back(v);
+  }
+};
+
+int obs_energies(Engine& eng, std::vector<SysState>& S) {
+  MDB_TRY(eng.force(mdb::FM_OBS, true));
+  return eng.get_states(S);
+}
+
+void copy_trace(const Trace& tr, int32_t* es, double* et, int64_t cap) {
+  for (size_t k = 0; k < tr.steps.size() && (int64_t)k < cap; ++k) {
+    if (es) es[k] = tr.steps[k];
+    if (et) et[k] = tr.u[k];
+  }
+}
+
+}  // namespace
+
+int mdb_fire_minimize(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
+                      double force_tol, int32_t max_steps, const mdb_fire_params_t* params,
+                      const mdb_options_t* opt, mdb_particle_t* frame_out,
+                      mdb_minimize_result_t* result, int32_t* energy_steps,
+                      double* energy_trace, int64_t trace_cap) {
+  if (!cfg || !frame || !params || !result || n <= 0)
+    return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (max_steps <= 0) return mdb::set_error(MDB_ERR_ARG, "EnergyMinimizer: max_steps must be positive.");
+  mdb_options_t o = opts_or_default(opt);
+  Engine eng(o);
+  SystemSpec spec;
+  spec.cfg = *cfg;
+  spec.frame.assign(frame, frame + n);
+  spec.kind = mdb::K_FIRE;
+  spec.fire = *params;
+  spec.tol = force_tol;
+  spec.max_steps = max_steps;
+  spec.fire_prepare = true;
+  MDB_TRY(eng.add_system(std::move(spec)));
+  MDB_TRY(eng.build());
+  Trace tr;
+  std::vector<SysState> S;
+  MDB_TRY(obs_energies(eng, S));
+  tr.add(0, S[0].U);
+  int64_t done = 0;
+  bool converged = false;
+  int32_t steps = max_steps;
+  while (done < max_steps) {
+    const int64_t to_sample = 1000 - (done % 1000);
+    const int64_t chunk = std::min<int64_t>(to_sample, (int64_t)max_steps - done);
+    MDB_TRY(eng.run_fire(chunk));
+    done += chunk;
+    MDB_TRY(eng.get_states(S));
+    if (S[0].f_conv) {
+      converged = true;
+      steps = S[0].f_conv_step;
+      MDB_TRY(obs_energies(eng, S));
+      tr.add(steps + 1, S[0].U);
+      break;
+    }
+    if (done % 1000 == 0) {
+      MDB_TRY(obs_energies(eng, S));
+      tr.add((int32_t)done, S[0].U);
+    }
+  }
+  if (!converged && (tr.steps.empty() || tr.steps.back() != max_steps)) {
+    MDB_TRY(obs_energies(eng, S));
+    tr.add(max_steps, S[0].U);
+  }
+  MDB_TRY(obs_energies(eng, S));
+  memset(result, 0, sizeof(*result));
+  result->steps = steps;
+  result->converged = converged ? 1 : 0;
+  result->max_force = S[0].f_maxf;
+  result->potential_energy = S[0].U;
+  result->n_energy_samples = (int64_t)tr.steps.size();
+  result->nonfinite = S[0].nonfinite;
+  copy_trace(tr, energy_steps, energy_trace, trace_cap);
+  if (frame_out) MDB_TRY(eng.get_frame(0, frame_out));
+  return MDB_OK;
+}
+
+// ------------------------------------------------------------- batches --
+
+}  // extern "C"
+
+struct mdb_batch {
+  mdb_options_t opt;
+  std::unique_ptr<Engine> eng;
+  std::vector<SystemSpec> pending;
+  std::vector<Trace> traces;
+  std::vector<int32_t> recorded_done;  // final sample recorded
+  std::vector<int32_t> max_steps;
+  int64_t iter = 0;
+  bool built = false;
+};
+
+namespace {
+
+int batch_build(mdb_batch_t* b) {
+  if (b->built) return MDB_OK;
+  if (b->pending.empty()) return mdb::set_error(MDB_ERR_STATE, "batch has no systems");
+  b->eng.reset(new Engine(b->opt));
+  const size_t ns = b->pending.size();
+  for (auto& s : b->pending) MDB_TRY(b->eng->add_system(std::move(s)));
+  b->pending.clear();
+  MDB_TRY(b->eng->build());
+  b->traces.assign(ns, Trace());
+  b->recorded_done.assign(ns, 0);
+  std::vector<SysState> S;
+  MDB_TRY(obs_energies(*b->eng, S));
+  for (size_t s = 0; s < ns; ++s) b->traces[s].add(0, S[s].U);
+  b->built = true;
+  return MDB_OK;
+}
+
+bool fire_finished(const SysState& S, int32_t max_steps) {
+  return S.f_conv != 0 || S.f_step >= max_steps || S.err != 0;
+}
+
+// Records convergence and periodic energy samples after a chunk that ended
+// at iteration b->iter.
+int batch_harvest(mdb_batch_t* b) {
+  std::vector<SysState> S;
+  MDB_TRY(b->eng->get_states(S));
+  bool need_u = false;
+  const size_t ns = S.size();
+  for (size_t s = 0; s < ns; ++s) {
+    if (b->recorded_done[s]) continue;
+    if (S[s].f_conv || S[s].f_step >= b->max_steps[s] || (b->iter % 1000 == 0)) need_u = true;
+  }
+  if (!need_u) return MDB_OK;
+  std::vector<SysState> U;
+  MDB_TRY(obs_energies(*b->eng, U));
+  for (size_t s = 0; s < ns; ++s) {
+    if (b->recorded_done[s]) continue;
+    Trace& tr = b->traces[s];
+    if (S[s].f_conv) {
+      tr.add(S[s].f_conv_step + 1, U[s].U);
+      b->recorded_done[s] = 1;
+    } else if (S[s].f_step >= b->max_steps[s]) {
+      if (tr.steps.empty() || tr.steps.back() != b->max_steps[s]) tr.add(b->max_steps[s], U[s].U);
+      b->recorded_done[s] = 1;
+    } else if (b->iter % 1000 == 0) {
+      tr.add((int32_t)b->iter, U[s].U);
+    }
+  }
+  return MDB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdb_batch_create(const mdb_options_t* opt, mdb_batch_t** out) {
+  if (!out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  mdb_batch_t* b = new (std::nothrow) mdb_batch();
+  if (!b) return mdb::set_error(MDB_ERR_CAPACITY, "out of host memory");
+  b->opt = opts_or_default(opt);
+  *out = b;
+  return MDB_OK;
+}
+
+int mdb_batch_destroy(mdb_batch_t* b) {
+  delete b;
+  return MDB_OK;
+}
+
+int mdb_batch_add_fire(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
+                       int64_t n, double force_tol, int32_t max_steps,
+                       const mdb_fire_params_t* params, int32_t* sys_id) {
+  if (!b || !cfg || !frame || !params || n <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (b->built) return mdb::set_error(MDB_ERR_STATE, "systems can only be added before the first run");
+  if (max_steps <= 0) return mdb::set_error(MDB_ERR_ARG, "max_steps must be positive");
+  SystemSpec spec;
+  spec.cfg = *cfg;
+  spec.frame.assign(frame, frame + n);
+  spec.kind = mdb::K_FIRE;
+  spec.fire = *params;
+  spec.tol = force_tol;
+  spec.max_steps = max_steps;
+  spec.fire_prepare = true;
+  b->pending.push_back(std::move(spec));
+  b->max_steps.push_back(max_steps);
+  if (sys_id) *sys_id = (int32_t)b->pending.size() - 1;
+  return MDB_OK;
+}
+
+int mdb_batch_add_md(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
+                     int64_t n, int32_t kind, int64_t nsteps, int32_t* sys_id) {
+  (void)b;
+  (void)cfg;
+  (void)frame;
+  (void)n;
+  (void)kind;
+  (void)nsteps;
+  (void)sys_id;
+  return mdb::set_error(MDB_ERR_STATE, "MD segments in batches are not available in this build");
+}
+
+int mdb_batch_run(mdb_batch_t* b, int64_t iterations) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  int32_t cap = 0;
+  for (int32_t m : b->max_steps) cap = m > cap ? m : cap;
+  int64_t left = iterations < 0 ? (int64_t)cap - b->iter : iterations;
+  while (left > 0 && b->iter < cap) {
+    const int64_t to_sample = 1000 - (b->iter % 1000);
+    const int64_t chunk = std::min<int64_t>(std::min<int64_t>(to_sample, left), (int64_t)cap - b->iter);
+    MDB_TRY(b->eng->run_fire(chunk));
+    b->iter += chunk;
+    left -= chunk;
+    MDB_TRY(batch_harvest(b));
+    bool all = true;
+    for (size_t s = 0; s < b->recorded_done.size(); ++s) all = all && b->recorded_done[s];
+    if (all) break;
+  }
+  return MDB_OK;
+}
+
+int mdb_batch_progress(mdb_batch_t* b, int32_t* n_systems, int32_t* n_done) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  const int32_t ns = b->built ? (int32_t)b->recorded_done.size() : (int32_t)b->pending.size();
+  int32_t d = 0;
+  if (b->built)
+    for (int32_t x : b->recorded_done) d += x ? 1 : 0;
+  if (n_systems) *n_systems = ns;
+  if (n_done) *n_done = d;
+  return MDB_OK;
+}
+
+int mdb_batch_system_info(mdb_batch_t* b, int32_t sys_id, int64_t* n, int32_t* done,
+                          int64_t* steps) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (sys_id < 0 || sys_id >= b->eng->nsys()) return mdb::set_error(MDB_ERR_ARG, "bad system id");
+  SysState S;
+  MDB_TRY(b->eng->get_state(sys_id, &S));
+  if (n) *n = b->eng->n(sys_id);
+  if (done) *done = fire_finished(S, b->max_steps[sys_id]) ? 1 : 0;
+  if (steps) *steps = S.f_conv ? S.f_conv_step : S.f_step;
+  return MDB_OK;
+}
+
+int mdb_batch_get_frame(mdb_batch_t* b, int32_t sys_id, mdb_particle_t* out, int64_t n) {
+  if (!b || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (sys_id < 0 || sys_id >= b->eng->nsys()) return mdb::set_error(MDB_ERR_ARG, "bad system id");
+  if (n != b->eng->n(sys_id)) return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the system size");
+  return b->eng->get_frame(sys_id, out);
+}
+
+int mdb_batch_get_fire_result(mdb_batch_t* b, int32_t sys_id, mdb_minimize_result_t* result,
+                              int32_t* energy_steps, double* energy_trace, int64_t trace_cap) {
+  if (!b || !result) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (sys_id < 0 || sys_id >= b->eng->nsys()) return mdb::set_error(MDB_ERR_ARG, "bad system id");
+  std::vector<SysState> U;
+  MDB_TRY(obs_energies(*b->eng, U));
+  const SysState& S = U[sys_id];
+  memset(result, 0, sizeof(*result));
+  result->converged = S.f_conv ? 1 : 0;
+  result->steps = S.f_conv ? S.f_conv_step : b->max_steps[sys_id];
+  result->max_force = S.f_maxf;
+  result->potential_energy = S.U;
+  result->n_energy_samples = (int64_t)b->traces[sys_id].steps.size();
+  result->nonfinite = S.nonfinite;
+  copy_trace(b->traces[sys_id], energy_steps, energy_trace, trace_cap);
+  return MDB_OK;
+}
+
+int mdb_batch_cuda_stream(mdb_batch_t* b, void** stream) {
+  if (!b || !stream) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  *stream = (void*)b->eng->stream();
+  return MDB_OK;
+}
+
+// ----------------------------------------------------- single-call kernels --
+
+int mdb_compute_forces(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
+                       double Lx, double Ly, int32_t periodic_y, const mdb_options_t* opt,
+                       double* acc_out, double* U_out, double* W_out) {
+  if (!cfg || !frame || n <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  mdb_options_t o = opts_or_default(opt);
+  Engine eng(o);
+  SystemSpec spec;
+  spec.cfg = *cfg;
+  spec.cfg.box_w_global = Lx;
+  spec.cfg.box_h_global = Ly;
+  spec.cfg.k_piston = 0.0;  // pair forces only
+  spec.frame.assign(frame, frame + n);
+  MDB_TRY(eng.add_system(std::move(spec)));
+  MDB_TRY(eng.build());
+  const bool py = periodic_y != 0;
+  if (!py) MDB_TRY(eng.rebuild_now(0));
+  MDB_TRY(eng.force(mdb::FM_INIT, py));
+  if (acc_out) {
+    std::vector<mdb_particle_t> f((size_t)n);
+    MDB_TRY(eng.get_frame(0, f.data()));
+    for (int64_t i = 0; i < n; ++i) {
+      acc_out[2 * i] = f[i].acc.x;
+      acc_out[2 * i + 1] = f[i].acc.y;
+    }
+  }
+  if (U_out || W_out) {
+    MDB_TRY(eng.force(mdb::FM_OBS, py));
+    SysState S;
+    MDB_TRY(eng.get_state(0, &S));
+    if (U_out) *U_out = S.U;
+    if (W_out) *W_out = S.Wv;
+  }
+  return eng.sync();
+}
+
+int mdb_cell_build(const double* pos, int64_t n, double Lx, double Ly, double cell_min,
+                   int32_t device, int32_t* cell_out, int32_t* perm_out, int32_t* ncx_out,
+                   int32_t* ncy_out) {
+  if (!pos || n <= 0 || !(cell_min > 0.0)) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  mdb_options_t o;
+  mdb_options_default(&o);
+  o.device = device;
+  o.skin = cell_min * 0.5;
+  Engine eng(o);
+  SystemSpec spec;
+  mdb_config_default(&spec.cfg);
+  spec.cfg.box_w_global = Lx;
+  spec.cfg.box_h_global = Ly;
+  spec.cfg.SIGMA_AA = spec.cfg.SIGMA_BB = spec.cfg.SIGMA_AB = 1.0;
+  spec.cfg.cutoff = cell_min * 0.5;  // r_cell = cutoff * sigma_max + skin = cell_min
+  spec.cfg.barostat_height_max_ratio = 1.0;
+  spec.frame.assign((size_t)n, mdb_particle_t{});
+  for (int64_t i = 0; i < n; ++i) {
+    spec.frame[i].pos.x = pos[2 * i];
+    spec.frame[i].pos.y = pos[2 * i + 1];
+  }
+  MDB_TRY(eng.add_system(std::move(spec)));
+  MDB_TRY(eng.build());
+  std::vector<int32_t> orig((size_t)n), cell((size_t)n);
+  MDB_TRY(eng.debug_cells(0, orig.data(), cell.data()));
+  for (int64_t k = 0; k < n; ++k) {
+    if (perm_out) perm_out[k] = orig[k];
+    if (cell_out) cell_out[orig[k]] = cell[k];
+  }
+  SysState S;
+  MDB_TRY(eng.get_state(0, &S));
+  if (ncx_out) *ncx_out = S.ncx;
+  if (ncy_out) *ncy_out = S.ncy;
+  return MDB_OK;
+}
+
+}  // extern "C"

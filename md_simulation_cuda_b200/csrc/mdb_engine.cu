@@ -1,0 +1,586 @@
+// Host engine of libmdb200 (see mdb_engine.h) and the kernel instantiations.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "mdb_engine.h"
+#include "mdb_kernels.cuh"
+#include "mdb_util.h"
+
+namespace mdb {
+
+namespace {
+
+void* force_fn(int fm, bool py) {
+#define MDB_F(M) return py ? (void*)k_force<M, true> : (void*)k_force<M, false>
+  switch (fm) {
+    case FM_INIT: MDB_F(FM_INIT);
+    case FM_NVE: MDB_F(FM_NVE);
+    case FM_NH: MDB_F(FM_NH);
+    case FM_NPH: MDB_F(FM_NPH);
+    case FM_PISTON: MDB_F(FM_PISTON);
+    case FM_FIRE: MDB_F(FM_FIRE);
+    default: MDB_F(FM_OBS);
+  }
+#undef MDB_F
+}
+
+void* drift_fn(int dm) {
+  switch (dm) {
+    case DM_NVE: return (void*)k_drift<DM_NVE>;
+    case DM_NH: return (void*)k_drift<DM_NH>;
+    case DM_NPH: return (void*)k_drift<DM_NPH>;
+    case DM_PISTON: return (void*)k_drift<DM_PISTON>;
+    default: return (void*)k_drift<DM_FIRE>;
+  }
+}
+
+double next_pow2(double x) {
+  double b = 1.0;
+  while (b < x) b *= 2.0;
+  return b;
+}
+
+}  // namespace
+
+Engine::Engine(const mdb_options_t& opt) {
+  device_ = opt.device;
+  skin_ = opt.skin > 0.0 ? opt.skin : 0.3;
+  use_graphs_ = opt.use_graphs != 0;
+}
+
+Engine::~Engine() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  drop_graphs();
+  for (void* p : allocs_) cudaFree(p);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::drop_graphs() {
+  for (auto& kv : graphs_) {
+    if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
+    if (kv.second.first) cudaGraphDestroy(kv.second.first);
+  }
+  graphs_.clear();
+}
+
+int Engine::ensure_device() {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return set_error(MDB_ERR_NODEVICE, "no CUDA device available");
+  if (device_ < 0 || device_ >= ndev) return set_error(MDB_ERR_ARG, "invalid CUDA device ordinal");
+  MDB_CUDA(cudaSetDevice(device_));
+  if (!stream_) MDB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  return MDB_OK;
+}
+
+int Engine::add_system(SystemSpec&& spec) {
+  if (built_) return set_error(MDB_ERR_STATE, "systems can only be added before build()");
+  if (spec.frame.empty()) return set_error(MDB_ERR_ARG, "a system needs at least one particle");
+  if (spec.frame.size() > (size_t)INT32_MAX / 2)
+    return set_error(MDB_ERR_CAPACITY, "too many particles in one system");
+  const mdb_config_t& c = spec.cfg;
+  if (!(c.box_w_global > 0.0) || !(c.box_h_global > 0.0) || !isfinite(c.box_w_global) ||
+      !isfinite(c.box_h_global))
+    return set_error(MDB_ERR_BOX, "box_w_global and box_h_global must be positive");
+  if (!(c.cutoff > 0.0) || !(c.dt > 0.0) || !isfinite(c.dt))
+    return set_error(MDB_ERR_CONFIG, "cutoff and dt must be positive");
+  if (!(c.MASS_A > 0.0) || !(c.MASS_B > 0.0))
+    return set_error(MDB_ERR_CONFIG, "MASS_A and MASS_B must be positive");
+  if (!(c.SIGMA_AA > 0.0) || !(c.SIGMA_BB > 0.0) || !(c.SIGMA_AB > 0.0))
+    return set_error(MDB_ERR_CONFIG, "SIGMA_* must be positive");
+  specs_.push_back(std::move(spec));
+  return MDB_OK;
+}
+
+int Engine::build() {
+  if (built_) return set_error(MDB_ERR_STATE, "engine already built");
+  if (specs_.empty()) return set_error(MDB_ERR_STATE, "no systems");
+  int rc = ensure_device();
+  if (rc) return rc;
+  const int ns = (int)specs_.size();
+  hsp_.resize(ns);
+  std::vector<SysState> hst(ns);
+  int64_t p0 = 0, c0 = 0;
+  int b0 = 0;
+  int64_t maxn = 0;
+  for (int s = 0; s < ns; ++s) {
+    const SystemSpec& sp = specs_[s];
+    const mdb_config_t& c = sp.cfg;
+    SysParams& P = hsp_[s];
+    memset(&P, 0, sizeof(P));
+    const int32_t n = (int32_t)sp.frame.size();
+    maxn = std::max<int64_t>(maxn, n);
+    P.p0 = p0;
+    P.n = n;
+    P.nb = (n + kThreads - 1) / kThreads;
+    P.b0 = b0;
+    P.kind = sp.kind;
+    P.sig[0] = c.SIGMA_AA;
+    P.sig[1] = c.SIGMA_BB;
+    P.sig[2] = c.SIGMA_AB;
+    P.eps[0] = c.EPSILON_AA;
+    P.eps[1] = c.EPSILON_BB;
+    P.eps[2] = c.EPSILON_AB;
+    const double inv_c = 1.0 / c.cutoff;
+    const double csr2 = inv_c * inv_c;
+    const double csr6 = csr2 * csr2 * csr2;
+    const double csr12 = csr6 * csr6;
+    const float cutoff_f = (float)c.cutoff;
+    for (int k = 0; k < 3; ++k) {
+      P.Vc[k] = P.eps[k] * (4.0 * (csr12 - csr6));
+      const float sf = (float)P.sig[k];
+      const float ef = (float)P.eps[k];
+      P.fsig2[k] = sf * sf;
+      P.feps24[k] = 24.0f * ef;
+      P.feps4[k] = 4.0f * ef;
+      const float rcf = cutoff_f * sf;
+      P.frc2[k] = rcf * rcf;
+    }
+    P.massA = c.MASS_A;
+    P.massB = c.MASS_B;
+    P.cutoff = c.cutoff;
+    P.rc_max = c.cutoff * std::max(P.sig[0], std::max(P.sig[1], P.sig[2]));
+    P.skin = skin_;
+    P.r_cell = P.rc_max + skin_;
+    P.dt = c.dt;
+    P.Q = c.Q;
+    P.T0 = c.T_target;
+    P.g_dof = 2.0 * (double)c.n_particles_global - 2.0;
+    P.W = c.barostat_mass > 1e-12 ? c.barostat_mass : 1e-12;
+    P.k_piston = c.k_piston;
+    P.hmin = c.barostat_height_min_ratio;
+    P.hmax = c.barostat_height_max_ratio;
+    P.Lx0 = c.box_w_global;
+    P.Ly0 = c.box_h_global;
+    P.rate_init = c.barostat_area_rate_init;
+    const double grow = std::max(1.0, P.hmax);
+    const double mx = 8.0 + 0.02 * P.Lx0, my = 8.0 + 0.02 * P.Ly0;
+    P.offx = next_pow2(grow * P.Lx0 + 2.0 * mx) + mx;
+    P.offy = next_pow2(grow * P.Ly0 + 2.0 * my) + my;
+    P.ccap_x = std::max(1, (int)floor(grow * P.Lx0 / P.r_cell) + 1);
+    P.ccap_y = std::max(1, (int)floor(grow * P.Ly0 / P.r_cell) + 1);
+    P.c0 = c0;
+    P.f_dt_max = sp.fire.dt_max;
+    P.f_alpha0 = sp.fire.alpha0;
+    P.f_inc = sp.fire.f_inc;
+    P.f_dec = sp.fire.f_dec;
+    P.f_Nmin = sp.fire.N_min;
+    P.f_tol = sp.tol;
+    P.f_max_steps = sp.max_steps;
+    P.target_steps = sp.target_steps;
+    SysState& S = hst[s];
+    memset(&S, 0, sizeof(S));
+    S.Lx = c.box_w_global;
+    S.Ly = c.box_h_global;
+    S.aspect = 1.0;
+    S.periodic_y = 1;
+    S.fl = std::max(1e-12, P.hmin * P.Ly0);
+    S.ce = std::max(S.fl, P.hmax * P.Ly0);
+    S.need_rebuild = 1;
+    S.ncx = S.ncy = 1;
+    S.allpairs = 1;
+    S.f_dt = sp.fire.dt_init;
+    S.f_alpha = sp.fire.alpha0;
+    p0 += n;
+    b0 += P.nb;
+    c0 += (int64_t)P.ccap_x * P.ccap_y;
+  }
+  ntot_ = p0;
+  nblocks_ = b0;
+  ncells_ = c0;
+  if (ntot_ >= (int64_t)INT32_MAX || ncells_ >= (int64_t)INT32_MAX)
+    return set_error(MDB_ERR_CAPACITY, "batch exceeds 2^31 particles or cells");
+
+  auto alloc = [&](void** p, size_t bytes) -> int {
+    MDB_CUDA(cudaMalloc(p, bytes < 16 ? 16 : bytes));
+    allocs_.push_back(*p);
+    return MDB_OK;
+  };
+#define MDB_ALLOC(ptr, count)                                                 \
+  do {                                                                        \
+    int rc_ = alloc((void**)&(ptr), sizeof(*(ptr)) * (size_t)(count));       \
+    if (rc_) return rc_;                                                      \
+  } while (0)
+  Dev& D = dev_;
+  memset(&D, 0, sizeof(D));
+  int32_t* sob;
+  int32_t* sid;
+  SysParams* dsp;
+  MDB_ALLOC(sob, nblocks_);
+  MDB_ALLOC(sid, ntot_);
+  MDB_ALLOC(dsp, ns);
+  D.sys_of_block = sob;
+  D.sysid = sid;
+  D.sp = dsp;
+  MDB_ALLOC(D.st, ns);
+  MDB_ALLOC(D.bg, 1);
+  MDB_ALLOC(D.pos, ntot_);
+  MDB_ALLOC(D.vel, ntot_);
+  MDB_ALLOC(D.acc, ntot_);
+  MDB_ALLOC(D.type, ntot_);
+  MDB_ALLOC(D.theta, ntot_);
+  MDB_ALLOC(D.orig, ntot_);
+  MDB_ALLOC(D.pos2, ntot_);
+  MDB_ALLOC(D.vel2, ntot_);
+  MDB_ALLOC(D.acc2, ntot_);
+  MDB_ALLOC(D.type2, ntot_);
+  MDB_ALLOC(D.theta2, ntot_);
+  MDB_ALLOC(D.orig2, ntot_);
+  MDB_ALLOC(D.pff, ntot_);
+  MDB_ALLOC(D.sb, ntot_);
+  MDB_ALLOC(D.cell_of, ntot_);
+  MDB_ALLOC(D.key, ntot_);
+  MDB_ALLOC(D.perm, ntot_);
+  MDB_ALLOC(D.ccount, ncells_);
+  MDB_ALLOC(D.ccursor, ncells_);
+  MDB_ALLOC(D.cstart, ncells_ + 1);
+  const int64_t ntiles = (ncells_ + kScanTile - 1) / kScanTile;
+  MDB_ALLOC(D.scan_part, ntiles + 1);
+  MDB_ALLOC(D.part, (int64_t)nblocks_ * kNP);
+  MDB_ALLOC(D.partm, (int64_t)nblocks_ * 4);
+  aos_cap_ = maxn;
+  {
+    int rc2 = alloc(&d_aos_, sizeof(mdb_particle_t) * (size_t)maxn);
+    if (rc2) return rc2;
+  }
+#undef MDB_ALLOC
+  D.nsys = ns;
+  D.nblocks = nblocks_;
+  D.ntot = ntot_;
+  D.ncells = ncells_;
+  D.use_cond = 0;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+  const int64_t work = std::max(ntot_, ncells_);
+  rb_grid_ = (int)std::min<int64_t>((work + kThreads - 1) / kThreads, (int64_t)nsm * 8);
+  rb_grid_ = std::max(rb_grid_, 1);
+  scan_grid_ = (int)std::min<int64_t>(ntiles, (int64_t)nsm * 4);
+  scan_grid_ = std::max(scan_grid_, 1);
+  D.rb_grid = rb_grid_;
+
+  // block table, per-slot system ids, parameters, state
+  std::vector<int32_t> hsob(nblocks_), hsid(ntot_);
+  for (int s = 0; s < ns; ++s) {
+    for (int b = 0; b < hsp_[s].nb; ++b) hsob[hsp_[s].b0 + b] = s;
+    for (int k = 0; k < hsp_[s].n; ++k) hsid[hsp_[s].p0 + k] = s;
+  }
+  MDB_CUDA(cudaMemcpyAsync(sob, hsob.data(), sizeof(int32_t) * hsob.size(),
+                           cudaMemcpyHostToDevice, stream_));
+  MDB_CUDA(cudaMemcpyAsync(sid, hsid.data(), sizeof(int32_t) * hsid.size(),
+                           cudaMemcpyHostToDevice, stream_));
+  MDB_CUDA(cudaMemcpyAsync(dsp, hsp_.data(), sizeof(SysParams) * ns, cudaMemcpyHostToDevice,
+                           stream_));
+  MDB_CUDA(cudaMemcpyAsync(D.st, hst.data(), sizeof(SysState) * ns, cudaMemcpyHostToDevice,
+                           stream_));
+  BatchGlobal bg{};
+  bg.nsys = ns;
+  MDB_CUDA(cudaMemcpyAsync(D.bg, &bg, sizeof(bg), cudaMemcpyHostToDevice, stream_));
+  MDB_CUDA(cudaMemsetAsync(D.part, 0, sizeof(double) * (size_t)nblocks_ * kNP, stream_));
+  MDB_CUDA(cudaMemsetAsync(D.partm, 0, sizeof(double) * (size_t)nblocks_ * 4, stream_));
+  MDB_CUDA(cudaMemsetAsync(D.cell_of, 0, sizeof(int32_t) * (size_t)ntot_, stream_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  built_ = true;
+  for (int s = 0; s < ns; ++s) {
+    rc = set_frame(s, specs_[s].frame.data());
+    if (rc) return rc;
+    if (specs_[s].fire_prepare) {
+      const int g = (int)std::min<int64_t>((hsp_[s].n + kThreads - 1) / kThreads, 1024);
+      k_fire_prepare<<<g, kThreads, 0, stream_>>>(dev_, hsp_[s].p0, hsp_[s].n, s);
+      MDB_CUDA(cudaGetLastError());
+      launches_ += 1;
+    }
+  }
+  return rebuild_now(-1);
+}
+
+int Engine::launch(void* fn, int grid, int block, const Dev& d) {
+  Dev copy = d;
+  void* args[] = {&copy};
+  MDB_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, stream_));
+  launches_ += 1;
+  count_launches(1);
+  return MDB_OK;
+}
+
+int Engine::launch_rebuild_eager() {
+  const Dev& d = dev_;
+  int rc;
+  if ((rc = launch((void*)k_rb_zero, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_bin, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_scan_tiles, scan_grid_, kScanBlock, d))) return rc;
+  if ((rc = launch((void*)k_scan_parts, 1, 1024, d))) return rc;
+  if ((rc = launch((void*)k_scan_add, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_scatter, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_cellsort, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_permute, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_copyback, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_finish, 1, kThreads, d))) return rc;
+  return MDB_OK;
+}
+
+int Engine::rebuild_now(int periodic_y) {
+  if (!built_) return set_error(MDB_ERR_STATE, "engine not built");
+  MDB_CUDA(cudaSetDevice(device_));
+  k_force_rebuild<<<1, kThreads, 0, stream_>>>(dev_, periodic_y);
+  MDB_CUDA(cudaGetLastError());
+  launches_ += 1;
+  count_launches(1);
+  return launch_rebuild_eager();
+}
+
+int Engine::set_pext(double p) {
+  MDB_CUDA(cudaSetDevice(device_));
+  k_set_pext<<<1, kThreads, 0, stream_>>>(dev_, p);
+  MDB_CUDA(cudaGetLastError());
+  launches_ += 1;
+  count_launches(1);
+  return MDB_OK;
+}
+
+int Engine::force(int fm, bool py) {
+  MDB_CUDA(cudaSetDevice(device_));
+  return launch(force_fn(fm, py), nblocks_, kThreads, dev_);
+}
+
+int Engine::reduce_K() {
+  MDB_CUDA(cudaSetDevice(device_));
+  return launch((void*)k_reduce_K, nblocks_, kThreads, dev_);
+}
+
+int Engine::add_kernel_node(cudaGraph_t g, const cudaGraphNode_t* deps, int ndeps, void* fn,
+                            int grid, int block, const Dev& d, cudaGraphNode_t* out) {
+  Dev copy = d;
+  void* args[] = {&copy};
+  cudaKernelNodeParams kp = {};
+  kp.func = fn;
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(block);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = args;
+  kp.extra = nullptr;
+  MDB_CUDA(cudaGraphAddKernelNode(out, g, deps, (size_t)ndeps, &kp));
+  return MDB_OK;
+}
+
+int Engine::add_rebuild_body(cudaGraph_t body, const Dev& d) {
+  struct K {
+    void* fn;
+    int grid, block;
+  } ks[] = {
+      {(void*)k_rb_zero, rb_grid_, kThreads},     {(void*)k_rb_bin, rb_grid_, kThreads},
+      {(void*)k_scan_tiles, scan_grid_, kScanBlock}, {(void*)k_scan_parts, 1, 1024},
+      {(void*)k_scan_add, rb_grid_, kThreads},    {(void*)k_rb_scatter, rb_grid_, kThreads},
+      {(void*)k_rb_cellsort, rb_grid_, kThreads}, {(void*)k_rb_permute, rb_grid_, kThreads},
+      {(void*)k_rb_copyback, rb_grid_, kThreads}, {(void*)k_rb_finish, 1, kThreads},
+  };
+  cudaGraphNode_t prev = nullptr;
+  for (const K& k : ks) {
+    cudaGraphNode_t node;
+    int rc = add_kernel_node(body, prev ? &prev : nullptr, prev ? 1 : 0, k.fn, k.grid, k.block, d,
+                             &node);
+    if (rc) return rc;
+    prev = node;
+  }
+  return MDB_OK;
+}
+
+int Engine::add_cond_rebuild(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                             cudaGraphNode_t* out) {
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  MDB_CUDA(cudaGraphAddNode(out, g, &dep, 1, &cp));
+  Dev d = dev_;
+  d.use_cond = 0;
+  return add_rebuild_body(cp.conditional.phGraph_out[0], d);
+}
+
+// kind 0: MD steps (drift, cond rebuild, force); kind 1: FIRE iterations
+// (force, drift, cond rebuild).
+int Engine::get_graph(int kind, int dm, int fm, bool py, int chunk, cudaGraphExec_t* exec) {
+  auto key = std::make_tuple(kind, dm, fm, py ? 1 : 0, chunk);
+  auto it = graphs_.find(key);
+  if (it != graphs_.end()) {
+    *exec = it->second.second;
+    return MDB_OK;
+  }
+  cudaGraph_t g;
+  MDB_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphNode_t prev = nullptr;
+  int rc = MDB_OK;
+  for (int k = 0; k < chunk && rc == MDB_OK; ++k) {
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) {
+      rc = cuda_error(e, "cudaGraphConditionalHandleCreate");
+      break;
+    }
+    Dev dd = dev_;
+    dd.cond = h;
+    dd.use_cond = 1;
+    cudaGraphNode_t nd, nc, nf;
+    if (kind == 0) {
+      rc = add_kernel_node(g, prev ? &prev : nullptr, prev ? 1 : 0, drift_fn(dm), nblocks_,
+                           kThreads, dd, &nd);
+      if (!rc) rc = add_cond_rebuild(g, nd, h, &nc);
+      if (!rc) rc = add_kernel_node(g, &nc, 1, force_fn(fm, py), nblocks_, kThreads, dev_, &nf);
+      prev = nf;
+    } else {
+      rc = add_kernel_node(g, prev ? &prev : nullptr, prev ? 1 : 0, force_fn(FM_FIRE, true),
+                           nblocks_, kThreads, dev_, &nf);
+      if (!rc) rc = add_kernel_node(g, &nf, 1, drift_fn(DM_FIRE), nblocks_, kThreads, dd, &nd);
+      if (!rc) rc = add_cond_rebuild(g, nd, h, &nc);
+      prev = nc;
+    }
+  }
+  if (rc != MDB_OK) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  cudaGraphExec_t ex;
+  cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_error(e, "cudaGraphInstantiate");
+  }
+  graphs_[key] = std::make_pair(g, ex);
+  *exec = ex;
+  return MDB_OK;
+}
+
+int Engine::run_md(int dm, int fm, bool py, int64_t nsteps) {
+  if (!built_) return set_error(MDB_ERR_STATE, "engine not built");
+  MDB_CUDA(cudaSetDevice(device_));
+  int64_t left = nsteps;
+  if (use_graphs_) {
+    static const int kChunks[] = {64, 8, 1};
+    for (int c : kChunks) {
+      while (left >= c) {
+        cudaGraphExec_t ex;
+        int rc = get_graph(0, dm, fm, py, c, &ex);
+        if (rc) {
+          use_graphs_ = false;  // fall back to eager launches
+          break;
+        }
+        MDB_CUDA(cudaGraphLaunch(ex, stream_));
+        launches_ += 2LL * c;
+        count_launches(2LL * c);
+        left -= c;
+      }
+      if (!use_graphs_) break;
+    }
+  }
+  for (; left > 0; --left) {
+    int rc;
+    if ((rc = launch(drift_fn(dm), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch_rebuild_eager())) return rc;
+    if ((rc = launch(force_fn(fm, py), nblocks_, kThreads, dev_))) return rc;
+  }
+  return MDB_OK;
+}
+
+int Engine::run_fire(int64_t iters) {
+  if (!built_) return set_error(MDB_ERR_STATE, "engine not built");
+  MDB_CUDA(cudaSetDevice(device_));
+  int64_t left = iters;
+  if (use_graphs_) {
+    static const int kChunks[] = {100, 10, 1};
+    for (int c : kChunks) {
+      while (left >= c) {
+        cudaGraphExec_t ex;
+        int rc = get_graph(1, DM_FIRE, FM_FIRE, true, c, &ex);
+        if (rc) {
+          use_graphs_ = false;
+          break;
+        }
+        MDB_CUDA(cudaGraphLaunch(ex, stream_));
+        launches_ += 2LL * c;
+        count_launches(2LL * c);
+        left -= c;
+      }
+      if (!use_graphs_) break;
+    }
+  }
+  for (; left > 0; --left) {
+    int rc;
+    if ((rc = launch(force_fn(FM_FIRE, true), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch(drift_fn(DM_FIRE), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch_rebuild_eager())) return rc;
+  }
+  return MDB_OK;
+}
+
+int Engine::get_state(int s, SysState* out) {
+  MDB_CUDA(cudaSetDevice(device_));
+  MDB_CUDA(cudaMemcpyAsync(out, dev_.st + s, sizeof(SysState), cudaMemcpyDeviceToHost, stream_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  return MDB_OK;
+}
+
+int Engine::get_states(std::vector<SysState>& out) {
+  MDB_CUDA(cudaSetDevice(device_));
+  out.resize(specs_.size());
+  MDB_CUDA(cudaMemcpyAsync(out.data(), dev_.st, sizeof(SysState) * out.size(),
+                           cudaMemcpyDeviceToHost, stream_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  return MDB_OK;
+}
+
+int Engine::put_state(int s, const SysState& st) {
+  MDB_CUDA(cudaSetDevice(device_));
+  MDB_CUDA(cudaMemcpyAsync(dev_.st + s, &st, sizeof(SysState), cudaMemcpyHostToDevice, stream_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  return MDB_OK;
+}
+
+int Engine::get_frame(int s, mdb_particle_t* out) {
+  MDB_CUDA(cudaSetDevice(device_));
+  const SysParams& P = hsp_[s];
+  const int g = (int)std::min<int64_t>((P.n + kThreads - 1) / kThreads, 4096);
+  k_export<<<g, kThreads, 0, stream_>>>(dev_, (DevParticle*)d_aos_, P.p0, P.n);
+  MDB_CUDA(cudaGetLastError());
+  launches_ += 1;
+  count_launches(1);
+  MDB_CUDA(cudaMemcpyAsync(out, d_aos_, sizeof(mdb_particle_t) * (size_t)P.n,
+                           cudaMemcpyDeviceToHost, stream_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  return MDB_OK;
+}
+
+int Engine::set_frame(int s, const mdb_particle_t* in) {
+  MDB_CUDA(cudaSetDevice(device_));
+  const SysParams& P = hsp_[s];
+  MDB_CUDA(cudaMemcpyAsync(d_aos_, in, sizeof(mdb_particle_t) * (size_t)P.n,
+                           cudaMemcpyHostToDevice, stream_));
+  const int g = (int)std::min<int64_t>((P.n + kThreads - 1) / kThreads, 4096);
+  k_import<<<g, kThreads, 0, stream_>>>(dev_, (const DevParticle*)d_aos_, P.p0, P.n);
+  MDB_CUDA(cudaGetLastError());
+  launches_ += 1;
+  count_launches(1);
+  return MDB_OK;
+}
+
+int Engine::debug_cells(int s, int32_t* orig, int32_t* cell) {
+  MDB_CUDA(cudaSetDevice(device_));
+  const SysParams& P = hsp_[s];
+  MDB_CUDA(cudaMemcpyAsync(orig, dev_.orig + P.p0, sizeof(int32_t) * (size_t)P.n,
+                           cudaMemcpyDeviceToHost, stream_));
+  MDB_CUDA(cudaMemcpyAsync(cell, dev_.cell_of + P.p0, sizeof(int32_t) * (size_t)P.n,
+                           cudaMemcpyDeviceToHost, stream_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  return MDB_OK;
+}
+
+int Engine::sync() {
+  MDB_CUDA(cudaSetDevice(device_));
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  return MDB_OK;
+}
+
+}  // namespace mdb

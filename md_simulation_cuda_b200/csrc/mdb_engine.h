@@ -1,0 +1,105 @@
+// Host engine: owns the device memory of a batch of independent systems (a
+// single simulation is a batch of one) and issues the step phases.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "mdb200.h"
+#include "mdb_internal.h"
+
+namespace mdb {
+
+struct SystemSpec {
+  mdb_config_t cfg;
+  std::vector<mdb_particle_t> frame;
+  int32_t kind = K_NVE;
+  mdb_fire_params_t fire{};
+  double tol = 0.0;
+  int32_t max_steps = 0;
+  int64_t target_steps = 0;
+  bool fire_prepare = false;  // wrap positions, zero v and a (FIRE entry)
+};
+
+class Engine {
+ public:
+  explicit Engine(const mdb_options_t& opt);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  int add_system(SystemSpec&& spec);
+  // Allocates and uploads every added system, then builds the cell lists.
+  int build();
+
+  int nsys() const { return (int)specs_.size(); }
+  int64_t n(int s) const { return (int64_t)specs_[s].frame.size(); }
+  const SysParams& params(int s) const { return hsp_[s]; }
+  cudaStream_t stream() const { return stream_; }
+  bool graphs() const { return use_graphs_; }
+  int device() const { return device_; }
+
+  // nsteps x { drift(dm) ; rebuild if needed ; force(fm) }
+  int run_md(int dm, int fm, bool py, int64_t nsteps);
+  // iters x { force(FIRE) ; drift(FIRE) ; rebuild if needed }
+  int run_fire(int64_t iters);
+  // One force-phase launch (FM_INIT / FM_OBS).
+  int force(int fm, bool py);
+  int reduce_K();
+  // Flags every system for a rebuild (periodic_y >= 0 also switches the y
+  // convention) and runs the rebuild pipeline now.
+  int rebuild_now(int periodic_y);
+  int set_pext(double p);
+
+  int get_state(int s, SysState* out);
+  int get_states(std::vector<SysState>& out);
+  int put_state(int s, const SysState& st);
+  int get_frame(int s, mdb_particle_t* out);
+  int set_frame(int s, const mdb_particle_t* in);
+  // Slot -> original index and slot -> local cell of system s (n entries each).
+  int debug_cells(int s, int32_t* orig, int32_t* cell);
+  int sync();
+
+  // Kernel launches issued (eager launches + kernel nodes of launched graphs,
+  // counting the rebuild body once per rebuild actually run).
+  long long launches_issued() const { return launches_; }
+
+ private:
+  int ensure_device();
+  int launch(void* fn, int grid, int block, const Dev& d);
+  int launch_rebuild_eager();
+  int add_kernel_node(cudaGraph_t g, const cudaGraphNode_t* deps, int ndeps, void* fn, int grid,
+                      int block, const Dev& d, cudaGraphNode_t* out);
+  int add_rebuild_body(cudaGraph_t body, const Dev& d);
+  int add_cond_rebuild(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                       cudaGraphNode_t* out);
+  int get_graph(int kind, int dm, int fm, bool py, int chunk, cudaGraphExec_t* exec);
+  void drop_graphs();
+
+  int device_ = 0;
+  double skin_ = 0.3;
+  bool use_graphs_ = true;
+  bool built_ = false;
+  cudaStream_t stream_ = nullptr;
+  std::vector<SystemSpec> specs_;
+  std::vector<SysParams> hsp_;
+  Dev dev_{};
+  int64_t ntot_ = 0, ncells_ = 0;
+  int nblocks_ = 0;
+  int rb_grid_ = 0;
+  int scan_grid_ = 0;
+  int64_t aos_cap_ = 0;
+  void* d_aos_ = nullptr;
+  std::vector<void*> allocs_;
+  std::map<std::tuple<int, int, int, int, int>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
+  long long launches_ = 0;
+  long long last_rebuilds_ = 0;
+};
+
+int reference_initial_frame(const mdb_config_t& cfg, std::vector<mdb_particle_t>& out);
+
+}  // namespace mdb

@@ -85,7 +85,7 @@ struct SysState {
   double f_dt, f_alpha, f_maxf, f_power;
   int32_t f_streak, f_conv, f_zero_v, f_step;
   int32_t f_conv_step;
-  int32_t pad_;
+  int32_t f_drift;  // the force phase of this iteration ran and did not converge
 };
 
 struct BatchGlobal {
@@ -119,7 +119,8 @@ struct Dev {
   int32_t* ccursor;
   int32_t* cstart;    // ncells + 1
   int32_t* scan_part; // per scan tile
-  double* part;       // nblocks * kNP
+  double* part;       // nblocks * kNP   block partial sums
+  double* partm;      // nblocks * 4     block partial maxima
   int32_t nsys;
   int32_t nblocks;
   int64_t ntot;

@@ -1,0 +1,1037 @@
+// Device code of libmdb200: sm_100a kernels for the LJ pair force, the fused
+// integrator phases, the reductions and the cell-list rebuild.
+//
+// Compiled with --fmad=false: every fused multiply-add is an explicit fma()/
+// fmaf(), so the FP64 integrator arithmetic is exactly the operation sequence
+// written here (the CPU oracle performs the same sequence).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "mdb_internal.h"
+
+namespace mdb {
+
+// ---------------------------------------------------------------- helpers --
+
+// pbc_wrap_hd (include/md_cuda_common.hpp:20-29).
+__device__ __forceinline__ double pbc_wrap(double x, double L) {
+  if (L <= 0.0) return x;
+  x = fmod(x, L);
+  if (x < 0.0) x += L;
+  return x;
+}
+
+// Type class for the parameter table (src/md_cuda_common.cu:218-229):
+// 0 -> A, 1 -> B, anything else -> "other" (pairs with it use AB).
+__device__ __forceinline__ int type_class(int t) { return t == 0 ? 0 : (t == 1 ? 1 : 2); }
+// Mass (src/md_cuda_common.cu:261): type 0 -> MASS_A, else MASS_B.
+__device__ __forceinline__ double type_mass(const SysParams& P, int t) {
+  return t == 0 ? P.massA : P.massB;
+}
+
+// Exact float-float split of a biased coordinate. X = x + off lies in one
+// binade [B, 2B), so the difference of two hi parts is exact; lo carries the
+// next 24 bits. The sign bits of the hi parts carry the type class
+// (x: class 1, y: class 2).
+__device__ __forceinline__ float4 encode_ff(double x, double y, int t, double offx, double offy) {
+  const double X = x + offx;
+  const double Y = y + offy;
+  float xh = __double2float_rn(X);
+  const float xl = __double2float_rn(X - (double)xh);
+  float yh = __double2float_rn(Y);
+  const float yl = __double2float_rn(Y - (double)yh);
+  const int tc = type_class(t);
+  if (tc == 1) xh = -xh;
+  if (tc == 2) yh = -yh;
+  return make_float4(xh, yh, xl, yl);
+}
+
+// Cell index along one axis: v = coordinate * (n / L); NaN and negatives
+// bin to 0, v >= n to n-1 (the oracle's or_cell_bin does the same).
+__device__ __forceinline__ int bin_axis(double v, int n) {
+  if (v >= 0.0 && v < (double)n) return (int)v;
+  if (v >= (double)n) return n - 1;
+  return 0;
+}
+
+__device__ __forceinline__ int grid_n(double L, double rcell, int cap) {
+  const double f = floor(L / rcell);
+  if (!(f >= 1.0)) return 1;
+  if (f >= (double)cap) return cap;
+  return (int)f;
+}
+
+// Compensated (Kahan) FP32 accumulation; the value is s - c.
+__device__ __forceinline__ void kahan(float& s, float& c, float x) {
+  const float y = x - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Fixed-order block reduction of kNP sums and 3 maxima (non-negative
+// values); valid in thread 0. The tree depends only on blockDim, so results
+// are bit-reproducible.
+__device__ __forceinline__ void block_reduce(double (&s)[kNP], double (&m)[3]) {
+  __shared__ double sh_s[kNP][kThreads / 32];
+  __shared__ double sh_m[3][kThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kNP; ++k) s[k] = warp_sum(s[k]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) m[k] = warp_max(m[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < kNP; ++k) sh_s[k][w] = s[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sh_m[k][w] = m[k];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < kNP; ++k) {
+      double v = lane < kThreads / 32 ? sh_s[k][lane] : 0.0;
+      s[k] = warp_sum(v);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double v = lane < kThreads / 32 ? sh_m[k][lane] : 0.0;
+      m[k] = warp_max(v);
+    }
+  }
+  __syncthreads();
+}
+
+// Publishes this block's partials (thread 0 holds them) and tells every
+// thread of the block whether it is the last of its system to finish.
+__device__ __forceinline__ bool publish_last(const Dev& D, SysState* S, int nb,
+                                             const double (&s)[kNP], const double (&m)[3]) {
+  __shared__ int am_last;
+  if (threadIdx.x == 0) {
+    double* p = D.part + (size_t)blockIdx.x * kNP;
+#pragma unroll
+    for (int k = 0; k < kNP; ++k) p[k] = s[k];
+    double* pm = D.partm + (size_t)blockIdx.x * 4;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) pm[k] = m[k];
+    __threadfence();
+    const unsigned prev = atomicAdd(&S->counter, 1u);
+    am_last = (prev == (unsigned)(nb - 1)) ? 1 : 0;
+  }
+  __syncthreads();
+  const bool last = am_last != 0;
+  if (last) __threadfence();
+  return last;
+}
+
+// Deterministic totals over the system's blocks (strided, then fixed tree).
+__device__ __forceinline__ void system_totals(const Dev& D, int b0, int nb, double (&s)[kNP],
+                                              double (&m)[3]) {
+#pragma unroll
+  for (int k = 0; k < kNP; ++k) s[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) m[k] = 0.0;
+  for (int b = threadIdx.x; b < nb; b += kThreads) {
+    const double* p = D.part + (size_t)(b0 + b) * kNP;
+    const double* pm = D.partm + (size_t)(b0 + b) * 4;
+#pragma unroll
+    for (int k = 0; k < kNP; ++k) s[k] += __ldcg(p + k);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) m[k] = fmax(m[k], __ldcg(pm + k));
+  }
+  block_reduce(s, m);
+}
+
+// Counts finished systems; the last one sets the graph condition for the
+// rebuild body from the batch-wide flag. Called by thread 0 of a system's
+// last block after its own state is final.
+__device__ __forceinline__ void system_done_and_signal(const Dev& D) {
+  __threadfence();
+  const unsigned prev = atomicAdd(&D.bg->sys_counter, 1u);
+  if (prev == (unsigned)(D.nsys - 1)) {
+    D.bg->sys_counter = 0u;
+    const int any = atomicOr(&D.bg->any_rebuild, 0);
+    if (D.use_cond) cudaGraphSetConditional(D.cond, any ? 1u : 0u);
+  }
+}
+
+// xi += 0.5 dt (2K - g T0) / Q (src/md_env.cu:1668-1673), host-order
+// arithmetic without contraction.
+__device__ __forceinline__ double nh_xi(const SysParams& P, double xi, double K) {
+  const double t1 = 0.5 * P.dt;
+  const double t2 = 2.0 * K;
+  const double t3 = P.g_dof * P.T0;
+  const double t4 = t2 - t3;
+  const double t5 = t1 * t4;
+  const double t6 = t5 / P.Q;
+  return xi + t6;
+}
+
+// --------------------------------------------------------- pair interaction --
+
+struct PairCtx {
+  float xih, yih, xil, yil;
+  float Lxh, Lxl, invLx, Lyh, Lyl, invLy;
+  uint32_t ts;  // class whose pairs with i use the "same" parameters
+  float rc2s, rc2ab, sig2s, sig2ab, e24s, e24ab, e4s, e4ab;
+  double Vcs, Vcab;
+};
+
+// The LJ pair term of li_force_kernel (src/md_cuda_common.cu:193-254) for the
+// candidates j in [j0, j1): exact float-float displacement with the nearest
+// image, strict cutoff 0 < r^2 < rc_ij^2 in FP32, FP32 pair force, Kahan FP32
+// accumulation. ENERGY adds 1/2 (u_ij - V_c) in FP64 (:795-807); VIRIAL adds
+// 1/2 r.F (:676-686) as the compensated FP32 sum of tmp*r^2.
+template <bool PY, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
+                                           const PairCtx& c, float& fxs, float& fxc, float& fys,
+                                           float& fyc, float& ws, float& wc, double& u) {
+#pragma unroll 4
+  for (int j = j0; j < j1; ++j) {
+    const float4 q = __ldg(pff + j);
+    float dxh = c.xih - fabsf(q.x);
+    const float sx = rintf(dxh * c.invLx);
+    dxh = fmaf(-sx, c.Lxh, dxh);
+    const float dx = dxh + fmaf(-sx, c.Lxl, c.xil - q.z);
+    float dyh = c.yih - fabsf(q.y);
+    float dy;
+    if (PY) {
+      const float sy = rintf(dyh * c.invLy);
+      dyh = fmaf(-sy, c.Lyh, dyh);
+      dy = dyh + fmaf(-sy, c.Lyl, c.yil - q.w);
+    } else {
+      dy = dyh + (c.yil - q.w);
+    }
+    const float r2 = fmaf(dx, dx, dy * dy);
+    const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
+    const bool same = (tj == c.ts);
+    const float rc2 = same ? c.rc2s : c.rc2ab;
+    if (r2 < rc2 && r2 > 0.0f) {
+      const float sig2 = same ? c.sig2s : c.sig2ab;
+      const float e24 = same ? c.e24s : c.e24ab;
+      const float r2i = __frcp_rn(r2);
+      const float sr2 = sig2 * r2i;
+      const float sr6 = sr2 * sr2 * sr2;
+      const float sr12 = sr6 * sr6;
+      const float tmp = e24 * fmaf(2.0f, sr12, -sr6) * r2i;
+      kahan(fxs, fxc, tmp * dx);
+      kahan(fys, fyc, tmp * dy);
+      if (VIRIAL) kahan(ws, wc, tmp * r2);
+      if (ENERGY) {
+        const float e4 = same ? c.e4s : c.e4ab;
+        const double vc = same ? c.Vcs : c.Vcab;
+        u = fma(0.5, (double)(e4 * (sr12 - sr6)) - vc, u);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void split_box(double L, float& h, float& l, float& inv) {
+  h = __double2float_rn(L);
+  l = __double2float_rn(L - (double)h);
+  inv = 1.0f / h;
+}
+
+// Sum of pair forces on slot i over its 3x3 cell stencil (or every slot of the
+// system for grids narrower than 3 cells). Returns F in FP64.
+template <bool PY, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
+                                               int64_t i, int ti, double Lx, double Ly,
+                                               double& fx, double& fy, double& w, double& u) {
+  PairCtx c;
+  const float4 qi = __ldg(D.pff + i);
+  c.xih = fabsf(qi.x);
+  c.yih = fabsf(qi.y);
+  c.xil = qi.z;
+  c.yil = qi.w;
+  split_box(Lx, c.Lxh, c.Lxl, c.invLx);
+  split_box(Ly, c.Lyh, c.Lyl, c.invLy);
+  const int tci = type_class(ti);
+  c.ts = (tci == 2) ? 99u : (uint32_t)tci;
+  const int sc = (tci == 2) ? 2 : tci;
+  c.rc2s = P.frc2[sc];
+  c.rc2ab = P.frc2[2];
+  c.sig2s = P.fsig2[sc];
+  c.sig2ab = P.fsig2[2];
+  c.e24s = P.feps24[sc];
+  c.e24ab = P.feps24[2];
+  c.e4s = P.feps4[sc];
+  c.e4ab = P.feps4[2];
+  c.Vcs = P.Vc[sc];
+  c.Vcab = P.Vc[2];
+  float fxs = 0.f, fxc = 0.f, fys = 0.f, fyc = 0.f, ws = 0.f, wc = 0.f;
+  u = 0.0;
+  const float4* __restrict__ pff = D.pff;
+  if (S.allpairs) {
+    pair_range<PY, ENERGY, VIRIAL>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
+                                   wc, u);
+  } else {
+    const int ncx = S.ncx, ncy = S.ncy;
+    const int cell = D.cell_of[i];
+    const int cx = cell % ncx, cy = cell / ncx;
+    const int* __restrict__ cs = D.cstart;
+#pragma unroll 1
+    for (int dr = -1; dr <= 1; ++dr) {
+      int yy = cy + dr;
+      if (PY) {
+        if (yy < 0) yy += ncy;
+        if (yy >= ncy) yy -= ncy;
+      } else if (yy < 0 || yy >= ncy) {
+        continue;
+      }
+      const int64_t row = P.c0 + (int64_t)yy * ncx;
+      if (cx > 0 && cx < ncx - 1) {
+        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + cx - 1), __ldg(cs + row + cx + 2), c,
+                                       fxs, fxc, fys, fyc, ws, wc, u);
+      } else if (cx == 0) {
+        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fxs, fxc, fys,
+                                       fyc, ws, wc, u);
+        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 1), __ldg(cs + row + ncx), c,
+                                       fxs, fxc, fys, fyc, ws, wc, u);
+      } else {
+        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 2), __ldg(cs + row + ncx), c,
+                                       fxs, fxc, fys, fyc, ws, wc, u);
+        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fxs, fxc,
+                                       fys, fyc, ws, wc, u);
+      }
+    }
+  }
+  fx = (double)fxs - (double)fxc;
+  fy = (double)fys - (double)fyc;
+  w = 0.5 * ((double)ws - (double)wc);
+}
+
+// Soft walls of piston_wall_kernel (src/md_cuda_common.cu:498-552) for one
+// particle: returns the y wall force and adds to the upper-wall force and the
+// wall energy.
+__device__ __forceinline__ double wall_terms(double y, double Ly, double k, double& up,
+                                             double& en) {
+  double wf = 0.0;
+  up = 0.0;
+  en = 0.0;
+  if (k > 0.0) {
+    if (y > Ly) {
+      const double ov = y - Ly;
+      wf = fma(-k, ov, wf);
+      up = fma(k, ov, up);
+      en = fma((0.5 * k) * ov, ov, en);
+    }
+    if (y < 0.0) {
+      const double ov = -y;
+      wf = fma(k, ov, wf);
+      en = fma((0.5 * k) * ov, ov, en);
+    }
+  }
+  return wf;
+}
+
+// ------------------------------------------------------------ force phase --
+// One thread per slot. FM selects what follows the force evaluation; PY is the
+// y image convention (false = the piston's walled y axis, which also applies
+// the soft walls in FM_INIT/FM_OBS).
+template <int FM, bool PY>
+__global__ void __launch_bounds__(kThreads) k_force(Dev D) {
+  const int b = blockIdx.x;
+  const int s = D.sys_of_block[b];
+  const SysParams& P = D.sp[s];
+  SysState* S = D.st + s;
+  const bool skip = (S->done != 0) || (S->err != 0) ||
+                    (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
+  const int64_t i = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+  const bool act = !skip && (i < P.p0 + P.n);
+  constexpr bool kEnergy = (FM == FM_OBS);
+  constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
+  double red[kNP];
+#pragma unroll
+  for (int k = 0; k < kNP; ++k) red[k] = 0.0;
+  double mx[3] = {0.0, 0.0, 0.0};
+  int bad = 0;
+  const double Lx = S->Lx, Ly = S->Ly;
+  const double dt = P.dt, h = 0.5 * dt;
+  if (act) {
+    const int ti = D.type[i];
+    double fx, fy, w, u;
+    particle_force<PY, kEnergy, kVirial>(D, P, *S, i, ti, Lx, Ly, fx, fy, w, u);
+    const double m = type_mass(P, ti);
+    double2 v = D.vel[i];
+    if (FM == FM_OBS) {
+      red[0] = u;
+      red[1] = w;
+      red[2] = m * fma(v.x, v.x, v.y * v.y);
+      if (!PY) {
+        double up, en;
+        wall_terms(D.pos[i].y, Ly, P.k_piston, up, en);
+        red[3] = up;
+        red[4] = en;
+      }
+    } else {
+      double ax = fx / m, ay = fy / m;
+      if (!PY && (FM == FM_INIT || FM == FM_PISTON)) {
+        double up, en;
+        const double wf = wall_terms(D.pos[i].y, Ly, P.k_piston, up, en);
+        if (wf != 0.0) ay = ay + wf / m;
+        red[0] = up;
+        red[1] = en;
+      }
+      if (FM == FM_NVE || FM == FM_PISTON) {
+        v.x = fma(h, ax, v.x);
+        v.y = fma(h, ay, v.y);
+      } else if (FM == FM_NH) {
+        const double xi2 = S->xi;
+        v.x = fma(h, fma(-xi2, v.x, ax), v.x);
+        v.y = fma(h, fma(-xi2, v.y, ay), v.y);
+        red[0] = (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+      } else if (FM == FM_NPH) {
+        red[0] = m * fma(v.x, v.x, v.y * v.y);
+        v.x = fma(h, ax, v.x);
+        v.y = fma(h, ay, v.y);
+        red[1] = m * fma(v.x, v.x, v.y * v.y);
+        red[2] = w;
+      } else if (FM == FM_FIRE) {
+        const double fdt = S->f_dt;
+        v.x = fma(fdt, ax, v.x);
+        v.y = fma(fdt, ay, v.y);
+        // ForceMag / PowerVal of reduce_force_metrics (src/md_energy_minimizer.cu:416-446)
+        const double fm = sqrt(fma(ax, ax, ay * ay));
+        if (fm != fm) {
+          mx[1] = 1.0;  // NaN |a|: never converged
+        } else {
+          mx[0] = fm;
+        }
+        red[0] = fma(v.x, ax, v.y * ay);
+      }
+      D.acc[i] = make_double2(ax, ay);
+      if (FM != FM_INIT) D.vel[i] = v;
+      if (!isfinite(ax) || !isfinite(ay) || !isfinite(v.x) || !isfinite(v.y)) bad = 1;
+    }
+  }
+  if (bad) atomicOr(&S->nonfinite, 1);
+  block_reduce(red, mx);
+  if (!publish_last(D, S, P.nb, red, mx)) return;
+  double tot[kNP];
+  double tmx[3];
+  system_totals(D, P.b0, P.nb, tot, tmx);
+  if (threadIdx.x != 0) return;
+  if (!skip) {
+    if (FM == FM_NH) {
+      S->K = tot[0];
+    } else if (FM == FM_NPH) {
+      const double A = Lx * Ly;
+      const double p_new = (A > 0.0) ? (tot[0] + tot[2]) / (2.0 * A) : 0.0;
+      double pA = S->pA + h * (p_new - S->p_ext);
+      if (S->clamped) {
+        if (Ly <= S->fl && pA < 0.0) pA = 0.0;
+        if (Ly >= S->ce && pA > 0.0) pA = 0.0;
+      }
+      S->pA = pA;
+      S->last_P = p_new;
+      S->P_cur = (A > 0.0) ? (tot[1] + tot[2]) / (2.0 * A) : 0.0;
+      S->Wv = tot[2];
+    } else if (FM == FM_PISTON) {
+      const double Fp = tot[0];
+      const double a_new = (Fp - S->p_ext * Lx) / P.W;
+      double vp = S->vp + h * a_new;
+      if (S->clamped) {
+        if (Ly <= S->fl && vp < 0.0) vp = 0.0;
+        if (Ly >= S->ce && vp > 0.0) vp = 0.0;
+      }
+      S->vp = vp;
+      S->Fp = Fp;
+      S->wallU = tot[1];
+      S->last_P = Fp / Lx;
+    } else if (FM == FM_INIT) {
+      if (!PY) {
+        S->Fp = tot[0];
+        S->wallU = tot[1];
+      }
+    } else if (FM == FM_OBS) {
+      S->U = tot[0];
+      S->Wv = tot[1];
+      S->kin = tot[2];
+      S->kin2 = tot[3];
+      S->wallU = tot[4];
+    } else if (FM == FM_FIRE) {
+      // FIRE control (src/md_energy_minimizer.cu:171-203)
+      const double maxf = (tmx[1] > 0.0) ? __longlong_as_double(0x7ff8000000000000ULL) : tmx[0];
+      S->f_power = tot[0];
+      S->f_maxf = maxf;
+      if (maxf < P.f_tol) {
+        S->f_conv = 1;
+        S->f_conv_step = S->f_step;
+      } else {
+        if (tot[0] > 0.0) {
+          S->f_streak += 1;
+          if (S->f_streak > P.f_Nmin) {
+            const double d2 = S->f_dt * P.f_inc;
+            S->f_dt = d2 < P.f_dt_max ? d2 : P.f_dt_max;
+            const double a2 = S->f_alpha * 0.99;
+            S->f_alpha = a2 > 0.0 ? a2 : 0.0;
+          }
+          S->f_zero_v = 0;
+        } else {
+          S->f_dt = S->f_dt * P.f_dec;
+          S->f_streak = 0;
+          S->f_alpha = P.f_alpha0;
+          S->f_zero_v = 1;
+        }
+        S->f_step += 1;
+      }
+    }
+    if (FM != FM_INIT && FM != FM_OBS && FM != FM_FIRE) S->steps += 1;
+  }
+  if (FM == FM_FIRE) S->f_drift = (!skip && !S->f_conv) ? 1 : 0;
+  S->counter = 0u;
+}
+
+// ------------------------------------------------------------ drift phase --
+// First half of a step for one slot: kick + drift + wrap (mode-specific),
+// float-float refresh, displacement since the last rebuild. The system's last
+// block applies the scalar updates and the rebuild criterion.
+template <int DMd>
+__global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
+  const int b = blockIdx.x;
+  const int s = D.sys_of_block[b];
+  const SysParams& P = D.sp[s];
+  SysState* S = D.st + s;
+  const bool skip = (S->done != 0) || (S->err != 0) || (DMd == DM_FIRE && S->f_drift == 0);
+  const int64_t i = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+  const double dt = P.dt, h = 0.5 * dt;
+  const double Lx_old = S->Lx, Ly_old = S->Ly;
+  double Lx = Lx_old, Ly = Ly_old;
+  const bool py = S->periodic_y != 0;
+  // ---- scalar prelude (identical in every block) ----
+  double xi1 = 0.0, lam = 1.0, vsc = 1.0, pA1 = 0.0, vp1 = 0.0, aspect = S->aspect;
+  int clamped = 0, boxbad = 0;
+  if (DMd == DM_NH) xi1 = nh_xi(P, S->xi, S->K);
+  if (DMd == DM_NPH) {
+    // step_single_NPH (src/md_env.cu:1795-1881)
+    const double A_old = Lx_old * Ly_old;
+    pA1 = S->pA + h * (S->P_cur - S->p_ext);
+    double A_new = A_old + dt * (pA1 / P.W);
+    if (!(A_old > 0.0) || !(A_new > 0.0) || !isfinite(A_new)) boxbad = 1;
+    if (!(aspect > 0.0) || !isfinite(aspect)) aspect = Lx_old / Ly_old;
+    double Ly_new = sqrt(A_new / aspect);
+    double Lx_new = aspect * Ly_new;
+    if (Ly_new < S->fl) {
+      Ly_new = S->fl;
+      Lx_new = aspect * Ly_new;
+      A_new = Lx_new * Ly_new;
+      clamped = 1;
+    } else if (Ly_new > S->ce) {
+      Ly_new = S->ce;
+      Lx_new = aspect * Ly_new;
+      A_new = Lx_new * Ly_new;
+      clamped = 1;
+    }
+    lam = sqrt(A_new / A_old);
+    vsc = 1.0 / lam;
+    if (Lx_new <= 0.0 || Ly_new <= 0.0) boxbad = 1;
+    Lx = Lx_new;
+    Ly = Ly_new;
+  }
+  if (DMd == DM_PISTON) {
+    // step_single_NPH_piston (src/md_env.cu:1939-1989)
+    if (Lx_old <= 0.0 || Ly_old <= 0.0) boxbad = 1;
+    const double a_old = (S->Fp - S->p_ext * Lx_old) / P.W;
+    vp1 = S->vp + h * a_old;
+    double Ly_new = Ly_old + dt * vp1;
+    if (Ly_new < S->fl) {
+      Ly_new = S->fl;
+      clamped = 1;
+      if (vp1 < 0.0) vp1 = 0.0;
+    } else if (Ly_new > S->ce) {
+      Ly_new = S->ce;
+      clamped = 1;
+      if (vp1 > 0.0) vp1 = 0.0;
+    }
+    Ly = Ly_new;
+  }
+  double fdt = 0.0, alpha = 0.0;
+  int zero_v = 0;
+  if (DMd == DM_FIRE) {
+    fdt = S->f_dt;
+    alpha = S->f_alpha;
+    zero_v = S->f_zero_v;
+  }
+  const bool act = !skip && !boxbad && (i < P.p0 + P.n);
+  double red[kNP];
+#pragma unroll
+  for (int k = 0; k < kNP; ++k) red[k] = 0.0;
+  double mx[3] = {0.0, 0.0, 0.0};
+  int bad = 0;
+  if (act) {
+    double2 x = D.pos[i];
+    double2 v = D.vel[i];
+    const double2 a = D.acc[i];
+    const int t = D.type[i];
+    const double m = type_mass(P, t);
+    const double2 x0 = x;
+    if (DMd == DM_NVE || DMd == DM_PISTON) {
+      // step_half_vv_kernel (src/md_cuda_common.cu:381-394), piston (:396-409)
+      v.x = fma(h, a.x, v.x);
+      v.y = fma(h, a.y, v.y);
+      x.x = fma(dt, v.x, x.x);
+      x.y = fma(dt, v.y, x.y);
+    } else if (DMd == DM_NH) {
+      // step_half_vv_nh_kernel (src/md_cuda_common.cu:454-478)
+      v.x = fma(h, fma(-xi1, v.x, a.x), v.x);
+      v.y = fma(h, fma(-xi1, v.y, a.y), v.y);
+      x.x = fma(dt, v.x, x.x);
+      x.y = fma(dt, v.y, x.y);
+      red[0] = (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+    } else if (DMd == DM_NPH) {
+      // step_half_nph_velocity_kernel + step_nph_scale_and_drift_kernel (:411-440)
+      v.x = fma(h, a.x, v.x);
+      v.y = fma(h, a.y, v.y);
+      v.x = v.x * vsc;
+      v.y = v.y * vsc;
+      x.x = fma(dt, v.x, lam * x.x);
+      x.y = fma(dt, v.y, lam * x.y);
+    } else if (DMd == DM_FIRE) {
+      // zero_velocity / fire_velocity_mix / drift (src/md_energy_minimizer.cu:32-71)
+      if (zero_v) {
+        v.x = 0.0;
+        v.y = 0.0;
+      } else {
+        const double vmag = sqrt(fma(v.x, v.x, v.y * v.y));
+        const double fmag = sqrt(fma(a.x, a.x, a.y * a.y));
+        if (vmag > 0.0 && fmag > 0.0) {
+          const double scale = vmag / fmag;
+          v.x = fma(alpha * scale, a.x, (1.0 - alpha) * v.x);
+          v.y = fma(alpha * scale, a.y, (1.0 - alpha) * v.y);
+        }
+      }
+      x.x = fma(fdt, v.x, x.x);
+      x.y = fma(fdt, v.y, x.y);
+    }
+    const double xu = x.x, yu = x.y;
+    x.x = pbc_wrap(x.x, Lx);
+    if (DMd != DM_PISTON) x.y = pbc_wrap(x.y, Ly);
+    D.pos[i] = x;
+    D.vel[i] = v;
+    D.pff[i] = encode_ff(x.x, x.y, t, P.offx, P.offy);
+    // displacement since the last rebuild and the single-step jump
+    const double ilx = 1.0 / Lx, ily = 1.0 / Ly;
+    const float2 sb = D.sb[i];
+    float dsx = (float)(x.x * ilx) - sb.x;
+    dsx -= rintf(dsx);
+    const double dxr = (double)fabsf(dsx) * Lx;
+    double dyr;
+    if (py && DMd != DM_PISTON) {
+      float dsy = (float)(x.y * ily) - sb.y;
+      dsy -= rintf(dsy);
+      dyr = (double)fabsf(dsy) * Ly;
+    } else {
+      dyr = fabs(x.y - (double)sb.y);
+    }
+    const double jx = fabs(xu * ilx - x0.x * (1.0 / Lx_old)) * Lx;
+    const double jy = (DMd == DM_PISTON) ? fabs(yu - x0.y) : fabs(yu * ily - x0.y * (1.0 / Ly_old)) * Ly;
+    mx[0] = dxr;
+    mx[1] = dyr;
+    mx[2] = fmax(jx, jy);
+    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(v.x) || !isfinite(v.y)) {
+      bad = 1;
+      mx[2] = __longlong_as_double(0x7ff0000000000000ULL);
+    }
+  }
+  if (bad) atomicOr(&S->nonfinite, 1);
+  block_reduce(red, mx);
+  if (!publish_last(D, S, P.nb, red, mx)) return;
+  double tot[kNP];
+  double tmx[3];
+  system_totals(D, P.b0, P.nb, tot, tmx);
+  if (threadIdx.x != 0) return;
+  if (!skip) {
+    if (boxbad) {
+      S->err = 5;  // MDB_ERR_BOX
+    } else {
+      if (DMd == DM_NH) {
+        S->xi = nh_xi(P, xi1, tot[0]);
+      } else if (DMd == DM_NPH) {
+        S->pA = pA1;
+        S->aspect = aspect;
+        S->Lx = Lx;
+        S->Ly = Ly;
+        S->clamped = clamped;
+      } else if (DMd == DM_PISTON) {
+        S->vp = vp1;
+        S->Ly = Ly;
+        S->clamped = clamped;
+      }
+      // rebuild criterion: a pair inside the cutoff now was within one cell
+      // width (per axis) at the last rebuild while 2*max displacement +
+      // rc_max stays below the current cell width.
+      const double slop = 1e-3 + 4e-7 * fmax(Lx, Ly);
+      const double wx = Lx / (double)S->ncx;
+      const double wy = (DMd == DM_PISTON) ? (S->Ly_b / (double)S->ncy) : Ly / (double)S->ncy;
+      int need = 0;
+      if (!S->allpairs) {
+        if (2.0 * tmx[0] + slop + P.rc_max >= wx) need = 1;
+        if (2.0 * tmx[1] + slop + P.rc_max >= wy) need = 1;
+        if (!(tmx[2] <= P.skin)) need = 1;  // large single-step moves, NaN
+      } else {
+        need = (!(tmx[2] <= 0.25 * fmin(Lx, Ly))) ? 1 : 0;
+      }
+      if (need) {
+        S->need_rebuild = 1;
+        atomicOr(&D.bg->any_rebuild, 1);
+      }
+    }
+  }
+  S->counter = 0u;
+  system_done_and_signal(D);
+}
+
+// K = sum 1/2 m |v|^2 (cal_local_K_kernel src/md_cuda_common.cu:554-589) into
+// S.K for every system.
+__global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
+  const int b = blockIdx.x;
+  const int s = D.sys_of_block[b];
+  const SysParams& P = D.sp[s];
+  SysState* S = D.st + s;
+  const int64_t i = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+  double red[kNP];
+#pragma unroll
+  for (int k = 0; k < kNP; ++k) red[k] = 0.0;
+  double mx[3] = {0.0, 0.0, 0.0};
+  if (i < P.p0 + P.n) {
+    const double2 v = D.vel[i];
+    const double m = type_mass(P, D.type[i]);
+    red[0] = (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+  }
+  block_reduce(red, mx);
+  if (!publish_last(D, S, P.nb, red, mx)) return;
+  double tot[kNP];
+  double tmx[3];
+  system_totals(D, P.b0, P.nb, tot, tmx);
+  if (threadIdx.x != 0) return;
+  S->K = tot[0];
+  S->counter = 0u;
+}
+
+// ------------------------------------------------------ cell-list rebuild --
+// All rebuild kernels are grid-stride with a fixed grid and return at once
+// when no system asked for a rebuild (the eager path launches them every step;
+// the graph path puts them behind a conditional node).
+
+__device__ __forceinline__ bool rebuild_requested(const Dev& D) {
+  return *((volatile int*)&D.bg->any_rebuild) != 0;
+}
+
+// System owning global cell c (cells of system s are [c0_s, c0_s + ccap_s)).
+__device__ __forceinline__ int cell_system(const Dev& D, int64_t c) {
+  int lo = 0, hi = D.nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (D.sp[mid].c0 <= c) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ bool sys_rebuilds(const Dev& D, int s) {
+  return *((volatile int*)&D.st[s].need_rebuild) != 0;
+}
+
+// Zero the cell counters of every system that rebuilds and compute its grid
+// for the current box. Systems that do not rebuild keep their counts, so the
+// global scan reproduces their cell ranges unchanged.
+__global__ void k_rb_zero(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t c = tid; c < D.ncells; c += stride) {
+    if (!sys_rebuilds(D, cell_system(D, c))) continue;
+    D.ccount[c] = 0;
+    D.ccursor[c] = 0;
+  }
+  for (int64_t s = tid; s < D.nsys; s += stride) {
+    if (!sys_rebuilds(D, (int)s)) continue;
+    const SysParams& P = D.sp[s];
+    SysState* S = D.st + s;
+    const double Lx = S->Lx, Ly = S->Ly;
+    const int ncx = grid_n(Lx, P.r_cell, P.ccap_x);
+    const int ncy = grid_n(Ly, P.r_cell, P.ccap_y);
+    S->ncx = ncx;
+    S->ncy = ncy;
+    S->allpairs = (ncx < 3 || (S->periodic_y && ncy < 3)) ? 1 : 0;
+    S->inv_wx = (double)ncx / Lx;
+    S->inv_wy = (double)ncy / Ly;
+    S->Lx_b = Lx;
+    S->Ly_b = Ly;
+  }
+}
+
+__global__ void k_rb_bin(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D.ntot; i += stride) {
+    const int s = D.sysid[i];
+    if (!sys_rebuilds(D, s)) continue;
+    const SysState* S = D.st + s;
+    const double2 p = D.pos[i];
+    const int ncx = S->ncx, ncy = S->ncy;
+    const int cx = bin_axis(p.x * S->inv_wx, ncx);
+    const int cy = bin_axis(p.y * S->inv_wy, ncy);
+    const int key = (int)(D.sp[s].c0 + (int64_t)cy * ncx + cx);
+    D.key[i] = key;
+    atomicAdd(D.ccount + key, 1);
+  }
+}
+
+// Exclusive scan of ccount into cstart: per-tile scan, scan of tile sums,
+// add. cstart[ncells] receives the total.
+__global__ void __launch_bounds__(kScanBlock) k_scan_tiles(Dev D) {
+  if (!rebuild_requested(D)) return;
+  __shared__ int sh[kScanBlock / 32];
+  const int64_t ntiles = (D.ncells + kScanTile - 1) / kScanTile;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t base = tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      v[k] = (base + k < D.ncells) ? D.ccount[base + k] : 0;
+      sum += v[k];
+    }
+    // block exclusive scan of per-thread sums
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int t = lane < kScanBlock / 32 ? sh[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      if (lane < kScanBlock / 32) sh[lane] = t;
+    }
+    __syncthreads();
+    int run = x - sum + (w > 0 ? sh[w - 1] : 0);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (base + k < D.ncells) D.cstart[base + k] = run;
+      run += v[k];
+    }
+    if (threadIdx.x == kScanBlock - 1) D.scan_part[tile] = run;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_parts(Dev D) {
+  if (!rebuild_requested(D)) return;
+  __shared__ int sh[32];
+  __shared__ int carry;
+  const int64_t ntiles = (D.ncells + kScanTile - 1) / kScanTile;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < ntiles; base += 1024) {
+    const int64_t k = base + threadIdx.x;
+    const int v = k < ntiles ? D.scan_part[k] : 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int t = sh[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      sh[lane] = t;
+    }
+    __syncthreads();
+    const int excl = x - v + (w > 0 ? sh[w - 1] : 0) + carry;
+    __syncthreads();
+    if (k < ntiles) D.scan_part[k] = excl;
+    if (threadIdx.x == 1023) carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) D.cstart[D.ncells] = carry;
+}
+
+__global__ void k_scan_add(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < D.ncells; c += stride)
+    D.cstart[c] += D.scan_part[c / kScanTile];
+}
+
+__global__ void k_rb_scatter(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D.ntot; i += stride) {
+    if (!sys_rebuilds(D, D.sysid[i])) continue;
+    const int key = D.key[i];
+    const int slot = D.cstart[key] + atomicAdd(D.ccursor + key, 1);
+    D.perm[slot] = (int)i;
+  }
+}
+
+// Within a cell the scatter order is arbitrary; sorting each cell's slots by
+// source slot makes the permutation the stable sort by cell.
+__global__ void k_rb_cellsort(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < D.ncells; c += stride) {
+    if (!sys_rebuilds(D, cell_system(D, c))) continue;
+    const int a = D.cstart[c], e = D.cstart[c + 1];
+    for (int k = a + 1; k < e; ++k) {
+      const int v = D.perm[k];
+      int q = k - 1;
+      while (q >= a && D.perm[q] > v) {
+        D.perm[q + 1] = D.perm[q];
+        --q;
+      }
+      D.perm[q + 1] = v;
+    }
+  }
+}
+
+__global__ void k_rb_permute(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < D.ntot; k += stride) {
+    const int s = D.sysid[k];
+    if (!sys_rebuilds(D, s)) continue;
+    const int src = D.perm[k];
+    const SysParams& P = D.sp[s];
+    const SysState* S = D.st + s;
+    const double2 p = D.pos[src];
+    const int t = D.type[src];
+    D.pos2[k] = p;
+    D.vel2[k] = D.vel[src];
+    D.acc2[k] = D.acc[src];
+    D.type2[k] = t;
+    D.theta2[k] = D.theta[src];
+    D.orig2[k] = D.orig[src];
+    D.cell_of[k] = (int)(D.key[src] - P.c0);
+    D.pff[k] = encode_ff(p.x, p.y, t, P.offx, P.offy);
+    const float sx = (float)(p.x * (1.0 / S->Lx));
+    const float sy = S->periodic_y ? (float)(p.y * (1.0 / S->Ly)) : (float)p.y;
+    D.sb[k] = make_float2(sx, sy);
+  }
+}
+
+__global__ void k_rb_copyback(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < D.ntot; k += stride) {
+    if (!sys_rebuilds(D, D.sysid[k])) continue;
+    D.pos[k] = D.pos2[k];
+    D.vel[k] = D.vel2[k];
+    D.acc[k] = D.acc2[k];
+    D.type[k] = D.type2[k];
+    D.theta[k] = D.theta2[k];
+    D.orig[k] = D.orig2[k];
+  }
+}
+
+__global__ void k_rb_finish(Dev D) {
+  if (!rebuild_requested(D)) return;
+  for (int s = threadIdx.x; s < D.nsys; s += blockDim.x) {
+    SysState* S = D.st + s;
+    if (!S->need_rebuild) continue;
+    S->need_rebuild = 0;
+    S->dmax_x = 0u;
+    S->dmax_y = 0u;
+    S->jump = 0u;
+    S->rebuilds += 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) D.bg->any_rebuild = 0;
+}
+
+// ------------------------------------------------------------ frame I/O --
+struct DevParticle {  // include/md_particle.hpp:31-38 (64 bytes)
+  double2 pos, vel, acc;
+  int32_t type, pad;
+  double theta;
+};
+
+__global__ void k_import(Dev D, const DevParticle* __restrict__ in, int64_t p0, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const DevParticle q = in[k];
+    const int64_t slot = p0 + k;
+    D.pos[slot] = q.pos;
+    D.vel[slot] = q.vel;
+    D.acc[slot] = q.acc;
+    D.type[slot] = q.type;
+    D.theta[slot] = q.theta;
+    D.orig[slot] = (int32_t)k;
+  }
+}
+
+// Wraps every position into the box (FIRE initialize_from_frame,
+// src/md_energy_minimizer.cu:386-419) and zeroes v and a when asked.
+__global__ void k_fire_prepare(Dev D, int64_t p0, int64_t n, int s) {
+  const SysState* S = D.st + s;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const int64_t slot = p0 + k;
+    double2 p = D.pos[slot];
+    p.x = pbc_wrap(p.x, S->Lx);
+    p.y = pbc_wrap(p.y, S->Ly);
+    D.pos[slot] = p;
+    D.vel[slot] = make_double2(0.0, 0.0);
+    D.acc[slot] = make_double2(0.0, 0.0);
+  }
+}
+
+__global__ void k_export(Dev D, DevParticle* __restrict__ out, int64_t p0, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const int64_t slot = p0 + k;
+    DevParticle q;
+    q.pos = D.pos[slot];
+    q.vel = D.vel[slot];
+    q.acc = D.acc[slot];
+    q.type = D.type[slot];
+    q.pad = 0;
+    q.theta = D.theta[slot];
+    out[D.orig[slot]] = q;
+  }
+}
+
+// Rebuild flag for every system (creation, frame import, mode switches).
+__global__ void k_force_rebuild(Dev D, int periodic_y) {
+  for (int s = threadIdx.x; s < D.nsys; s += blockDim.x) {
+    D.st[s].need_rebuild = 1;
+    if (periodic_y >= 0) D.st[s].periodic_y = periodic_y;
+  }
+  if (threadIdx.x == 0) D.bg->any_rebuild = 1;
+}
+
+__global__ void k_set_pext(Dev D, double p) {
+  for (int s = threadIdx.x; s < D.nsys; s += blockDim.x) D.st[s].p_ext = p;
+}
+
+}  // namespace mdb

@@ -1,0 +1,94 @@
+"""FIRE minimiser parity (EnergyMinimizer::minimize_frame) and batching."""
+import numpy as np
+import pytest
+
+import md_simulation_cuda_b200 as mdb
+from md_simulation_cuda_b200 import workloads as wl
+from oracle import pyoracle as po
+from tests.helpers import min_image, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _mgr(**kw):
+    m = mdb.MDConfigManager()
+    for k, v in kw.items():
+        setattr(m.config, k, v)
+    return m
+
+
+def test_two_particle_smoke(built):
+    """The reference's RUN_MINIMIZER_SMOKE case (tests/run_test/run_test.cpp:
+    107-148): 2 particles at (1,1), (3,1), box 10x10, tol 1e-3, 200 steps."""
+    mgr = _mgr(box_w_global=10.0, box_h_global=10.0, dt=1e-3, cutoff=2.5, SIGMA_BB=1.0,
+               SIGMA_AB=1.0, EPSILON_AB=1.0, n_particles_global=2, n_local=2, n_cap=16,
+               THREADS_PER_BLOCK=128, rank_size=1)
+    f = mdb.make_frame(2)
+    f["pos"] = [[1.0, 1.0], [3.0, 1.0]]
+    params = mdb.FireParams.from_config(mgr)
+    res = mdb.EnergyMinimizer(mgr).minimize_frame(f, 1e-3, 200, params)
+    cfgd = dict(SIGMA_AA=1.0, SIGMA_BB=1.0, SIGMA_AB=1.0, EPSILON_AA=1.0, EPSILON_BB=1.0,
+                EPSILON_AB=1.0, MASS_A=1.0, MASS_B=1.0, cutoff=2.5)
+    ref = po.fire_minimize(cfgd, f["pos"], f["type"], 10.0, 10.0, 1e-3, 200,
+                           dict(dt_init=1e-3, dt_max=5e-3, alpha0=0.1, f_inc=1.1, f_dec=0.5,
+                                N_min=5), mode=po.OR_FP64)
+    assert res.steps == ref["steps"] and res.converged == ref["converged"]
+    assert rel_err(res.max_force, ref["max_force"]) < 1e-5
+    assert np.abs(res.frame["pos"] - ref["pos"]).max() < 1e-7
+    assert res.energy_steps == ref["energy_steps"]
+
+
+def test_minimizer_errors(built):
+    mgr = _mgr(box_w_global=10.0, box_h_global=10.0, n_cap=0)
+    with pytest.raises(RuntimeError):
+        mdb.EnergyMinimizer(mgr)
+    mgr.config.n_cap = 1
+    em = mdb.EnergyMinimizer(mgr)
+    with pytest.raises(RuntimeError):
+        em.minimize_frame(mdb.make_frame(2), 1e-3, 10, mdb.FireParams.from_config(mgr))
+    with pytest.raises(RuntimeError):
+        em.minimize_frame(mdb.make_frame(1), 1e-3, 0, mdb.FireParams.from_config(mgr))
+
+
+def test_fire_lattice_quench_vs_oracle(built):
+    """A jittered lattice relaxes to its nearby minimum: final energy and
+    positions agree with the FP64 oracle."""
+    f, Lx, Ly = wl.lattice_frame(400, 0.9, 1.0, 0.6, 0.0, seed=61, jitter=0.2)
+    cfgd = wl.config_dict(400, Lx, Ly, dt=0.001)
+    mgr = mdb.MDConfigManager(mdb._lib.MDBConfigC())
+    for k, v in cfgd.items():
+        setattr(mgr.config, k, v)
+    mgr.config.n_cap = 1000
+    params = mdb.FireParams(dt_init=0.001, dt_max=0.01)
+    res = mdb.EnergyMinimizer(mgr).minimize_frame(f, 1e-4, 3000, params)
+    ref = po.fire_minimize(cfgd, f["pos"], f["type"], Lx, Ly, 1e-4, 3000,
+                           dict(dt_init=0.001, dt_max=0.01, alpha0=0.1, f_inc=1.1, f_dec=0.5,
+                                N_min=5), mode=po.OR_FP64)
+    assert res.converged and ref["converged"]
+    assert rel_err(res.potential_energy, ref["potential_energy"]) < 1e-6
+    d = min_image(res.frame["pos"] - ref["pos"], np.array([Lx, Ly]))
+    assert np.abs(d).max() < 1e-3
+
+
+def test_batch_equals_solo(built):
+    """Each system of a batch gives bit-identical results to running it alone
+    (per-system cell rebuilds, reductions and FIRE control)."""
+    systems = wl.fire_mix(6, seed=9, n_min=64, n_max=900)
+    params = mdb.FireParams(dt_init=0.001, dt_max=0.01)
+    b = mdb.Batch()
+    for f, cfgd in systems:
+        b.add_fire(cfgd, f, 1e-6, 400, params)
+    b.run()
+    n, done = b.progress()
+    assert n == 6 and done == 6
+    for k, (f, cfgd) in enumerate(systems):
+        mgr = mdb.MDConfigManager(mdb._lib.MDBConfigC())
+        for kk, v in cfgd.items():
+            setattr(mgr.config, kk, v)
+        mgr.config.n_cap = len(f)
+        solo = mdb.EnergyMinimizer(mgr).minimize_frame(f, 1e-6, 400, params)
+        rb = b.fire_result(k)
+        assert rb.steps == solo.steps and rb.converged == solo.converged
+        assert rb.max_force == solo.max_force
+        assert np.array_equal(rb.frame["pos"], solo.frame["pos"])
+        assert rb.energy_trace == solo.energy_trace
