@@ -1,0 +1,340 @@
+"""Benchmark of the MD stepping path: particle-steps/s.
+
+Default workload: the Nose-Hoover interface slab, N = 1,048,576 (Lx = 2 Ly at
+density 0.8, 90%/10% A stripes, T = 0.7, Q = 1.0, dt = 0.002), FP32 pair terms
+with FP64 state. A "step" is one step_single_nose_hoover() of that system.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload nvt_slab|nve_4096|fire_mix]
+
+Multi-GPU (torchrun, one rank per GPU): a single system does not shard, so
+every rank advances its own replica (seeded per rank) — weak scaling, no
+collective on the data path; time is the max over ranks.
+
+--impl reference times the reference's algorithm for this path on the host
+cores: its O(N^2) all-pairs force loop (src/md_cuda_common.cu:151-264) in the
+reference's mixed precision, restated by the CPU oracle, on a bounded sample of
+rows per step (the reference's CUDA build needs MPI and RAFT and cannot be
+built here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 1024 * 1024
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 lanes x FMA x 1.965 GHz
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if parts[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(name, rank):
+    from md_simulation_cuda_b200 import workloads as wl
+
+    if name == "nve_4096":
+        f, cfg = wl.nve_4096(seed=1 + 1000 * rank)
+        return f, cfg, "nve", "NVE velocity Verlet N=4096, rho=0.8, dt=0.001"
+    f, cfg = wl.nvt_slab(seed=2 + 1000 * rank)
+    return f, cfg, "nh", ("Nose-Hoover interface slab N=1048576, Lx=2Ly, rho=0.8, "
+                          "90%/10% A stripes, T=0.7, Q=1.0, dt=0.002")
+
+
+def cpu_cell_baseline(f, cfg, mode_name, budget_s=20.0):
+    """The oracle's cell-list step on all host cores (the fair CPU baseline)."""
+    from oracle import pyoracle as po
+
+    s = po.Sim(cfg, f["pos"], f["vel"], f["type"], mode=po.OR_REF_MIXED, use_cells=True)
+    step = s.step_nose_hoover if mode_name == "nh" else s.step_nve
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s / 2 or n >= 50:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": len(f) * n / dt, "unit": "particle-steps/s", "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": f"{n} full steps of the oracle's cell-list Nose-Hoover/NVE step "
+                      f"(reference mixed-precision pair arithmetic, OpenMP on all cores)"}
+
+
+def run_reference(args):
+    """Reference arm: the O(N^2) all-pairs force loop, bounded row sample."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from oracle import pyoracle as po
+
+    f, cfg, mode, desc = make_workload(args.workload, 0)
+    N = len(f)
+    Lx, Ly = cfg["box_w_global"], cfg["box_h_global"]
+    cores = os.cpu_count()
+    # calibrate rows/s, then size each step for ~budget/(K+W) seconds
+    t0 = time.perf_counter()
+    po.forces_rows(cfg, f["pos"], f["type"], Lx, Ly, 0, 16)
+    rate = 16 / (time.perf_counter() - t0)
+    budget = 90.0
+    rows = max(8, min(N, int(rate * budget / max(1, args.steps + args.warmup))))
+    for w in range(args.warmup):
+        po.forces_rows(cfg, f["pos"], f["type"], Lx, Ly, (w * rows) % (N - rows + 1), rows)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        po.forces_rows(cfg, f["pos"], f["type"], Lx, Ly, (k * rows) % (N - rows + 1), rows)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt
+    out = {"impl": "reference", "metric": "particle-steps/s", "value": value,
+           "unit": "particle-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "fp32-pair/fp64-accumulate", "data": "synthetic",
+           "config": {"workload": desc, "N": N},
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                            "kind": "port",
+                            "sample": f"{rows} rows of the O(N^2) force loop over all {N} "
+                                      f"particles per step (rows x 1 step = particle-steps)"},
+           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import md_simulation_cuda_b200 as mdb
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        dist = None
+    dev = local if ws > 1 else 0
+    torch.cuda.set_device(dev)
+    f, cfg, mode, desc = make_workload(args.workload, rank)
+    N = len(f)
+    sim = mdb.MDSimulation(cfg, frame=f, device=dev)
+    step = (lambda n: sim.step_single_nose_hoover(nsteps=n)) if mode == "nh" else \
+        (lambda n: sim.step_single_NVE(nsteps=n))
+    stream = torch.cuda.ExternalStream(sim.cuda_stream(), device=dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    step(args.warmup)
+    sim.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-timed region: K steps, L2 flushed between steps -------------
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    o0 = sim.observables()
+    l0 = mdb.kernel_launches()
+    barrier()
+    torch.cuda.synchronize(dev)
+    sim.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # evict the state from L2 (outside the step's events)
+            ev[k][0].record(stream)
+        step(1)
+        ev[k][1].record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    o1 = sim.observables()
+    launches = mdb.kernel_launches() - l0 + 10 * (o1.rebuilds - o0.rebuilds)
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t_local = t_ms / 1e3
+    if dist is not None:
+        t = torch.tensor([t_local], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    else:
+        t_max = t_local
+    value = N * ws * args.steps / t_max
+
+    # ---- the dominant kernel: per-phase CUDA events on the launching stream --
+    nph = 20
+    ms = sim.phase_times(nph, nose_hoover=(mode == "nh"))
+    t_force = ms[2] / nph / 1e3
+    t_drift = ms[0] / nph / 1e3
+    hbm_peak, peak_kind = _peaks()
+    force_bytes = 65.0 * N   # read pos(ff) 16 + type 1 + vel 16; write acc 16 + vel 16
+    step_bytes = 97.0 * N    # per particle-step, whole step
+    prof = os.path.join(ROOT, "profiles", "force_kernel_traffic.json")
+    traffic = None
+    if os.path.exists(prof):
+        pj = json.load(open(prof))
+        traffic = pj.get("dram_bytes_per_particle", None)
+        traffic = traffic * N if traffic else None
+    from oracle import pyoracle as po
+
+    p_ord = None
+    cpu = None
+    if rank == 0 and ws == 1:
+        p_ord = po.count_pairs_cells(cfg, f["pos"], f["type"], cfg["box_w_global"],
+                                     cfg["box_h_global"]) / N
+        cpu = cpu_cell_baseline(f, cfg, mode)
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    K2 = max(10, args.steps // 2)
+    pinned = torch.empty(N * 64, dtype=torch.uint8, pin_memory=True)
+    host = pinned.numpy().view(mdb.PARTICLE_DTYPE)
+    host[:] = f
+    out_pinned = torch.empty(N * 64, dtype=torch.uint8, pin_memory=True)
+    out_host = out_pinned.numpy().view(mdb.PARTICLE_DTYPE)
+    barrier()
+    sim.synchronize()
+    t0 = time.perf_counter()
+    sim.set_frame(host)                      # H2D of the step inputs
+    for _ in range(K2):
+        step(1)
+        _ = sim.observables()                # D2H of the step's result
+    mdb._lib.check(mdb._lib.lib().mdb_sim_get_frame(sim._h, mdb._lib.frame_ptr(out_host), N))
+    e2e_t = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e = {"value": N * ws * K2 / e2e_t, "unit": "particle-steps/s",
+           "h2d_bytes_per_step": int(64 * N / K2) + 8,
+           "d2h_bytes_per_step": int(64 * N / K2) + 112,
+           "steps": K2,
+           "how": "set_frame from pinned host memory, K steps each followed by an "
+                  "observables read, get_frame; wall clock"}
+
+    if rank == 0:
+        achieved = force_bytes / t_force / 1e9
+        out = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32-pair/fp64-state", "data": "synthetic (seeded jittered lattice)",
+            "config": {"workload": desc, "N": N, "parallelism": f"replicas x{ws}",
+                       "l2": "flushed between timed steps (256 MiB write outside the events)"},
+            "roofline": {"bound": "hbm", "kernel": "k_force<FM_NH> (pair force + NH kick + K)",
+                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "peak_source": peak_kind,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_particle": 65,
+                         "force_ms": t_force * 1e3, "drift_ms": t_drift * 1e3,
+                         "step_GBps_97B": step_bytes * value / ws / N / 1e9 if N else None,
+                         "fp32": {"achieved_tflops": (24.0 * p_ord * N / t_force / 1e12)
+                                  if p_ord else None,
+                                  "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_source": "nominal",
+                                  "pairs_per_particle": p_ord}},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    del sim
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="nvt_slab", choices=["nvt_slab", "nve_4096"])
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

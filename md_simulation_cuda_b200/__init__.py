@@ -256,6 +256,13 @@ class MDSimulation:
     def synchronize(self) -> None:
         check(lib().mdb_sim_synchronize(self._h))
 
+    def phase_times(self, nsteps: int, nose_hoover: bool = True):
+        """Summed (drift, rebuild, force) milliseconds of nsteps eager steps,
+        from CUDA events on this handle's stream."""
+        out = (C.c_double * 3)()
+        check(lib().mdb_sim_phase_times(self._h, 2 if nose_hoover else 1, int(nsteps), out))
+        return tuple(out)
+
     def cuda_stream(self) -> int:
         p = C.c_void_p()
         check(lib().mdb_sim_cuda_stream(self._h, C.byref(p)))

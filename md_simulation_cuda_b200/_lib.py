@@ -182,6 +182,7 @@ SIGNATURES = {
     "mdb_sim_get_config": ([_vp, _cfgp], C.c_int),
     "mdb_sim_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
     "mdb_sim_synchronize": ([_vp], C.c_int),
+    "mdb_sim_phase_times": ([_vp, C.c_int32, C.c_int64, _dp], C.c_int),
     "mdb_fire_params_from_config": ([_cfgp, C.POINTER(MDBFireParams)], C.c_int),
     "mdb_fire_minimize": ([_cfgp, _vp, C.c_int64, C.c_double, C.c_int32, C.POINTER(MDBFireParams),
                            _optp, _vp, C.POINTER(MDBMinimizeResult), _ip, _dp, C.c_int64], C.c_int),

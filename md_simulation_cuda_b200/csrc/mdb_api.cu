@@ -319,6 +319,24 @@ int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream) {
   return MDB_OK;
 }
 
+int mdb_sim_phase_times(mdb_sim_t* sim, int32_t kind, int64_t nsteps, double* ms_out) {
+  if (!sim || !ms_out || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (kind != MDB_JOB_NVE && kind != MDB_JOB_NVT)
+    return mdb::set_error(MDB_ERR_ARG, "kind must be MDB_JOB_NVE or MDB_JOB_NVT");
+  MDB_TRY(leave_piston(sim));
+  if (kind == MDB_JOB_NVT) {
+    if (!sim->k_valid) MDB_TRY(sim->eng->reduce_K());
+    MDB_TRY(sim->eng->run_md_timed(mdb::DM_NH, mdb::FM_NH, true, nsteps, ms_out));
+    sim->k_valid = true;
+  } else {
+    MDB_TRY(sim->eng->run_md_timed(mdb::DM_NVE, mdb::FM_NVE, true, nsteps, ms_out));
+    sim->k_valid = false;
+  }
+  sim->p_valid = false;
+  advance_time(sim, nsteps);
+  return MDB_OK;
+}
+
 int mdb_sim_synchronize(mdb_sim_t* sim) {
   if (!sim) return mdb::set_error(MDB_ERR_ARG, "null argument");
   MDB_TRY(sim->eng->sync());

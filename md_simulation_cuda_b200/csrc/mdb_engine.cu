@@ -1,5 +1,6 @@
 // Host engine of libmdb200 (see mdb_engine.h) and the kernel instantiations.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -48,6 +49,10 @@ Engine::Engine(const mdb_options_t& opt) {
   device_ = opt.device;
   skin_ = opt.skin > 0.0 ? opt.skin : 0.3;
   use_graphs_ = opt.use_graphs != 0;
+  // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
+  // see kernel nodes of graphs that contain conditional nodes).
+  const char* eager = getenv("MDB_EAGER");
+  if (eager && eager[0] == '1') use_graphs_ = false;
 }
 
 Engine::~Engine() {
@@ -483,6 +488,37 @@ int Engine::run_md(int dm, int fm, bool py, int64_t nsteps) {
     if ((rc = launch(force_fn(fm, py), nblocks_, kThreads, dev_))) return rc;
   }
   return MDB_OK;
+}
+
+int Engine::run_md_timed(int dm, int fm, bool py, int64_t nsteps, double* ms) {
+  if (!built_) return set_error(MDB_ERR_STATE, "engine not built");
+  MDB_CUDA(cudaSetDevice(device_));
+  cudaEvent_t ev[4];
+  for (int k = 0; k < 4; ++k) MDB_CUDA(cudaEventCreate(&ev[k]));
+  double acc[3] = {0.0, 0.0, 0.0};
+  int rc = MDB_OK;
+  for (int64_t s = 0; s < nsteps && rc == MDB_OK; ++s) {
+    cudaEventRecord(ev[0], stream_);
+    rc = launch(drift_fn(dm), nblocks_, kThreads, dev_);
+    cudaEventRecord(ev[1], stream_);
+    if (!rc) rc = launch_rebuild_eager();
+    cudaEventRecord(ev[2], stream_);
+    if (!rc) rc = launch(force_fn(fm, py), nblocks_, kThreads, dev_);
+    cudaEventRecord(ev[3], stream_);
+    cudaError_t e = cudaEventSynchronize(ev[3]);
+    if (e != cudaSuccess) {
+      rc = cuda_error(e, "cudaEventSynchronize");
+      break;
+    }
+    for (int k = 0; k < 3; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 4; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k];
+  return rc;
 }
 
 int Engine::run_fire(int64_t iters) {

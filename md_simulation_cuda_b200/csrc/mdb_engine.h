@@ -45,6 +45,9 @@ class Engine {
 
   // nsteps x { drift(dm) ; rebuild if needed ; force(fm) }
   int run_md(int dm, int fm, bool py, int64_t nsteps);
+  // Same steps issued eagerly with CUDA events around each phase on the
+  // engine's stream; ms[0..2] receive the summed drift / rebuild / force time.
+  int run_md_timed(int dm, int fm, bool py, int64_t nsteps, double* ms);
   // iters x { force(FIRE) ; drift(FIRE) ; rebuild if needed }
   int run_fire(int64_t iters);
   // One force-phase launch (FM_INIT / FM_OBS).

@@ -339,6 +339,79 @@ int or_forces_cells(const or_lj_t* lj, int64_t n, const double* pos, const int32
   return 0;
 }
 
+int or_forces_rows(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
+                   double Lx, double Ly, int32_t periodic_y, int32_t mode, int64_t row0,
+                   int64_t nrows, double* acc_rows, int32_t nthreads) {
+  if (row0 < 0 || nrows < 0 || row0 + nrows > n) return 1;
+  set_threads(nthreads);
+  const float Lx_f = (float)Lx, Ly_f = (float)Ly;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t r = 0; r < nrows; ++r) {
+    const int64_t i = row0 + r;
+    pair_acc_t a = {0.0, 0.0, 0.0, 0.0};
+    const double xi = pos[2 * i], yi = pos[2 * i + 1];
+    const int ti = type[i];
+    for (int64_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      do_pair(lj, mode, xi, yi, ti, pos[2 * j], pos[2 * j + 1], type[j], Lx, Ly, Lx_f, Ly_f,
+              periodic_y, &a);
+    }
+    const double m = type_mass(lj, ti);
+    acc_rows[2 * r] = a.fx / m;
+    acc_rows[2 * r + 1] = a.fy / m;
+  }
+  return 0;
+}
+
+int64_t or_count_pairs_cells(const or_lj_t* lj, int64_t n, const double* pos,
+                             const int32_t* type, double Lx, double Ly, int32_t nthreads) {
+  double smax = lj->sigma[0];
+  if (lj->sigma[1] > smax) smax = lj->sigma[1];
+  if (lj->sigma[2] > smax) smax = lj->sigma[2];
+  int32_t ncx, ncy;
+  or_cell_grid(Lx, Ly, lj->cutoff * smax, &ncx, &ncy);
+  if (ncx < 3 || ncy < 3) return or_count_pairs(lj, n, pos, type, Lx, Ly, 1, nthreads);
+  set_threads(nthreads);
+  const int32_t ncells = ncx * ncy;
+  int32_t* cell = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  int32_t* start = (int32_t*)malloc(sizeof(int32_t) * (size_t)(ncells + 1));
+  if (!cell || !perm || !start) {
+    free(cell);
+    free(perm);
+    free(start);
+    return -1;
+  }
+  or_cell_bin(n, pos, Lx, Ly, ncx, ncy, cell);
+  or_cell_sort(n, cell, ncells, perm, start);
+  int64_t total = 0;
+#pragma omp parallel for reduction(+ : total) schedule(dynamic, 256)
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t cx = cell[i] % ncx, cy = cell[i] / ncx;
+    for (int dyc = -1; dyc <= 1; ++dyc) {
+      const int32_t yy = (cy + dyc + ncy) % ncy;
+      for (int dxc = -1; dxc <= 1; ++dxc) {
+        const int32_t xx = (cx + dxc + ncx) % ncx;
+        const int32_t c = yy * ncx + xx;
+        for (int32_t k = start[c]; k < start[c + 1]; ++k) {
+          const int32_t j = perm[k];
+          if (j == i) continue;
+          double dx = pos[2 * i] - pos[2 * j], dy = pos[2 * i + 1] - pos[2 * j + 1];
+          dx = dx - Lx * round(dx / Lx);
+          dy = dy - Ly * round(dy / Ly);
+          const double rc = lj->cutoff * lj->sigma[pair_class(type[i], type[j])];
+          const double r2 = dx * dx + dy * dy;
+          if (r2 > 0.0 && r2 < rc * rc) total += 1;
+        }
+      }
+    }
+  }
+  free(cell);
+  free(perm);
+  free(start);
+  return total;
+}
+
 int64_t or_count_pairs(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
                        double Lx, double Ly, int32_t periodic_y, int32_t nthreads) {
   set_threads(nthreads);

@@ -61,6 +61,15 @@ int or_forces_allpairs(const or_lj_t* lj, int64_t n, const double* pos, const in
 int or_forces_cells(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
                     double Lx, double Ly, int32_t periodic_y, int32_t mode, double* acc,
                     double* U, double* W, int32_t nthreads);
+/* The all-pairs loop of li_force_kernel for the rows [row0, row0+nrows)
+ * only (acc_rows: 2*nrows doubles). A bounded sample of the reference's
+ * O(N^2) force pass, used as the timed CPU baseline. */
+int or_forces_rows(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
+                   double Lx, double Ly, int32_t periodic_y, int32_t mode, int64_t row0,
+                   int64_t nrows, double* acc_rows, int32_t nthreads);
+/* Ordered in-cutoff pairs counted through a cell list (large systems). */
+int64_t or_count_pairs_cells(const or_lj_t* lj, int64_t n, const double* pos,
+                             const int32_t* type, double Lx, double Ly, int32_t nthreads);
 /* Number of ordered pairs (i != j) inside their cutoff (FP64 test). */
 int64_t or_count_pairs(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
                        double Lx, double Ly, int32_t periodic_y, int32_t nthreads);

@@ -117,6 +117,12 @@ def lib():
             L.or_count_pairs.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
                                          C.c_double, C.c_int32, C.c_int32]
             L.or_count_pairs.restype = C.c_int64
+            L.or_count_pairs_cells.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
+                                               C.c_double, C.c_int32]
+            L.or_count_pairs_cells.restype = C.c_int64
+            L.or_forces_rows.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
+                                         C.c_double, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
+                                         dp, C.c_int32]
             L.or_cell_grid.argtypes = [C.c_double, C.c_double, C.c_double, ip, ip]
             L.or_cell_bin.argtypes = [C.c_int64, dp, C.c_double, C.c_double, C.c_int32,
                                       C.c_int32, ip]
@@ -194,6 +200,28 @@ def count_pairs(cfg, pos, types, Lx, Ly, periodic_y=1, nthreads=0):
     lj = make_lj(cfg)
     return int(lib().or_count_pairs(C.byref(lj), p.shape[0], _dp(p), _ip(t), Lx, Ly, periodic_y,
                                     nthreads))
+
+
+def count_pairs_cells(cfg, pos, types, Lx, Ly, nthreads=0):
+    p = _pos2(pos)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    lj = make_lj(cfg)
+    return int(lib().or_count_pairs_cells(C.byref(lj), p.shape[0], _dp(p), _ip(t), Lx, Ly,
+                                          nthreads))
+
+
+def forces_rows(cfg, pos, types, Lx, Ly, row0, nrows, periodic_y=1, mode=OR_REF_MIXED,
+                nthreads=0):
+    """acc of rows [row0, row0+nrows) through the all-pairs loop."""
+    p = _pos2(pos)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    acc = np.zeros((nrows, 2))
+    lj = make_lj(cfg)
+    rc = lib().or_forces_rows(C.byref(lj), p.shape[0], _dp(p), _ip(t), Lx, Ly, periodic_y, mode,
+                              row0, nrows, _dp(acc), nthreads)
+    if rc != 0:
+        raise RuntimeError("oracle forces_rows failed")
+    return acc
 
 
 def cell_build(pos, Lx, Ly, cell_min):
