@@ -108,7 +108,9 @@ typedef struct mdb_options {
   int32_t device;     /* CUDA device ordinal (default 0)                    */
   double skin;        /* cell-list skin in sigma units (default 0.3)        */
   int32_t use_graphs; /* 1: replay captured CUDA graphs for step chunks     */
-  int32_t reserved[13];
+  int32_t max_neighbors; /* neighbour-list capacity per particle (default 48;
+                            -1: no lists, always scan the cell stencil)     */
+  int32_t reserved[12];
 } mdb_options_t;
 
 /* MDConfig{} value-initialised defaults (include/md_config.hpp:14-75). */

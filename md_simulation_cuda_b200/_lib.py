@@ -98,7 +98,8 @@ class MDBOptions(C.Structure):
         ("device", C.c_int32),
         ("skin", C.c_double),
         ("use_graphs", C.c_int32),
-        ("reserved", C.c_int32 * 13),
+        ("max_neighbors", C.c_int32),
+        ("reserved", C.c_int32 * 12),
     ]
 
 
@@ -237,13 +238,15 @@ def check(rc: int):
     return rc
 
 
-def options(device=0, skin=None, use_graphs=True) -> MDBOptions:
+def options(device=0, skin=None, use_graphs=True, max_neighbors=None) -> MDBOptions:
     o = MDBOptions()
     lib().mdb_options_default(C.byref(o))
     o.device = device
     if skin is not None:
         o.skin = float(skin)
     o.use_graphs = 1 if use_graphs else 0
+    if max_neighbors is not None:
+        o.max_neighbors = int(max_neighbors)
     return o
 
 

@@ -578,6 +578,7 @@ void mdb_options_default(mdb_options_t* out) {
   out->device = 0;
   out->skin = 0.3;
   out->use_graphs = 1;
+  out->max_neighbors = 48;
 }
 
 }  // extern "C"

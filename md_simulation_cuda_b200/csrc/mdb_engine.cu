@@ -49,6 +49,7 @@ Engine::Engine(const mdb_options_t& opt) {
   device_ = opt.device;
   skin_ = opt.skin > 0.0 ? opt.skin : 0.3;
   use_graphs_ = opt.use_graphs != 0;
+  max_nbr_ = opt.max_neighbors > 0 ? opt.max_neighbors : (opt.max_neighbors < 0 ? 0 : 48);
   // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
   // see kernel nodes of graphs that contain conditional nodes).
   const char* eager = getenv("MDB_EAGER");
@@ -112,6 +113,12 @@ int Engine::build() {
   int64_t p0 = 0, c0 = 0;
   int b0 = 0;
   int64_t maxn = 0;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+  // A block covers kThreads * items slots of one system; large systems take
+  // several particles per thread so that one wave of ~4 blocks per SM covers
+  // them (fewer block partials, a short reduction tail).
+  const int64_t wave = (int64_t)nsm * 4 * kThreads;
   for (int s = 0; s < ns; ++s) {
     const SystemSpec& sp = specs_[s];
     const mdb_config_t& c = sp.cfg;
@@ -121,7 +128,8 @@ int Engine::build() {
     maxn = std::max<int64_t>(maxn, n);
     P.p0 = p0;
     P.n = n;
-    P.nb = (n + kThreads - 1) / kThreads;
+    P.items = (int)std::min<int64_t>(16, std::max<int64_t>(1, (n + wave - 1) / wave));
+    P.nb = (n + kThreads * P.items - 1) / (kThreads * P.items);
     P.b0 = b0;
     P.kind = sp.kind;
     P.sig[0] = c.SIGMA_AA;
@@ -151,6 +159,10 @@ int Engine::build() {
     P.rc_max = c.cutoff * std::max(P.sig[0], std::max(P.sig[1], P.sig[2]));
     P.skin = skin_;
     P.r_cell = P.rc_max + skin_;
+    for (int k = 0; k < 3; ++k) {
+      const double rl = c.cutoff * P.sig[k] + skin_;
+      P.frl2[k] = (float)(rl * rl);
+    }
     P.dt = c.dt;
     P.Q = c.Q;
     P.T0 = c.T_target;
@@ -240,6 +252,9 @@ int Engine::build() {
   MDB_ALLOC(D.cell_of, ntot_);
   MDB_ALLOC(D.key, ntot_);
   MDB_ALLOC(D.perm, ntot_);
+  D.max_nbr = max_nbr_;
+  MDB_ALLOC(D.ncount, ntot_);
+  if (max_nbr_ > 0) MDB_ALLOC(D.nlist, (int64_t)max_nbr_ * ntot_);
   MDB_ALLOC(D.ccount, ncells_);
   MDB_ALLOC(D.ccursor, ncells_);
   MDB_ALLOC(D.cstart, ncells_ + 1);
@@ -258,8 +273,6 @@ int Engine::build() {
   D.ntot = ntot_;
   D.ncells = ncells_;
   D.use_cond = 0;
-  int nsm = 148;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
   const int64_t work = std::max(ntot_, ncells_);
   rb_grid_ = (int)std::min<int64_t>((work + kThreads - 1) / kThreads, (int64_t)nsm * 8);
   rb_grid_ = std::max(rb_grid_, 1);
@@ -323,6 +336,7 @@ int Engine::launch_rebuild_eager() {
   if ((rc = launch((void*)k_rb_cellsort, rb_grid_, kThreads, d))) return rc;
   if ((rc = launch((void*)k_rb_permute, rb_grid_, kThreads, d))) return rc;
   if ((rc = launch((void*)k_rb_copyback, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_nlist, rb_grid_, kThreads, d))) return rc;
   if ((rc = launch((void*)k_rb_finish, 1, kThreads, d))) return rc;
   return MDB_OK;
 }
@@ -380,7 +394,8 @@ int Engine::add_rebuild_body(cudaGraph_t body, const Dev& d) {
       {(void*)k_scan_tiles, scan_grid_, kScanBlock}, {(void*)k_scan_parts, 1, 1024},
       {(void*)k_scan_add, rb_grid_, kThreads},    {(void*)k_rb_scatter, rb_grid_, kThreads},
       {(void*)k_rb_cellsort, rb_grid_, kThreads}, {(void*)k_rb_permute, rb_grid_, kThreads},
-      {(void*)k_rb_copyback, rb_grid_, kThreads}, {(void*)k_rb_finish, 1, kThreads},
+      {(void*)k_rb_copyback, rb_grid_, kThreads}, {(void*)k_rb_nlist, rb_grid_, kThreads},
+      {(void*)k_rb_finish, 1, kThreads},
   };
   cudaGraphNode_t prev = nullptr;
   for (const K& k : ks) {

@@ -85,6 +85,7 @@ class Engine {
 
   int device_ = 0;
   double skin_ = 0.3;
+  int max_nbr_ = 48;
   bool use_graphs_ = true;
   bool built_ = false;
   cudaStream_t stream_ = nullptr;

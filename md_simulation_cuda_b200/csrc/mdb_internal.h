@@ -50,8 +50,10 @@ struct SysParams {
   int32_t n;      // particles
   int32_t b0;     // first block of the block table
   int32_t nb;     // blocks
+  int32_t items;  // particles per thread (a block covers kThreads*items slots)
   int32_t ccap_x, ccap_y;
   int32_t kind;
+  float frl2[3];  // neighbour-list radius^2 per pair class: (rc_ij + skin)^2
   double sig[3], eps[3], Vc[3];  // AA, BB, AB
   double massA, massB, cutoff, rc_max, r_cell, skin;
   double dt, Q, T0, g_dof, W, k_piston, hmin, hmax, Lx0, Ly0, rate_init;
@@ -75,6 +77,7 @@ struct SysState {
   int32_t ncx, ncy, allpairs, periodic_y;
   int32_t clamped, nph_init, piston_active, piston_init;
   uint32_t dmax_x, dmax_y, jump;      // float bits (non-negative)
+  int32_t nl_overflow;                // particles whose list overflowed at the last rebuild
   int32_t need_rebuild;
   int32_t nonfinite;
   int32_t err;
@@ -115,6 +118,9 @@ struct Dev {
   int32_t* cell_of;
   int32_t* key;
   int32_t* perm;
+  int32_t* nlist;     // neighbour list, entry k of slot i at nlist[k * ntot + i]
+  int32_t* ncount;    // list length per slot, -1: use the cell stencil
+  int32_t max_nbr;
   int32_t* ccount;
   int32_t* ccursor;
   int32_t* cstart;    // ncells + 1

@@ -192,53 +192,80 @@ struct PairCtx {
   double Vcs, Vcab;
 };
 
-// The LJ pair term of li_force_kernel (src/md_cuda_common.cu:193-254) for the
-// candidates j in [j0, j1): exact float-float displacement with the nearest
-// image, strict cutoff 0 < r^2 < rc_ij^2 in FP32, FP32 pair force, Kahan FP32
-// accumulation. ENERGY adds 1/2 (u_ij - V_c) in FP64 (:795-807); VIRIAL adds
-// 1/2 r.F (:676-686) as the compensated FP32 sum of tmp*r^2.
+// Displacement i - j with the nearest image: the hi parts of two coordinates
+// in the same binade subtract exactly, the image shift s*L_hi is exact, the lo
+// parts carry the remaining bits, one rounding at the end.
+template <bool PY>
+__device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float& dx, float& dy) {
+  float dxh = c.xih - fabsf(q.x);
+  const float sx = rintf(dxh * c.invLx);
+  dxh = fmaf(-sx, c.Lxh, dxh);
+  dx = dxh + fmaf(-sx, c.Lxl, c.xil - q.z);
+  float dyh = c.yih - fabsf(q.y);
+  if (PY) {
+    const float sy = rintf(dyh * c.invLy);
+    dyh = fmaf(-sy, c.Lyh, dyh);
+    dy = dyh + fmaf(-sy, c.Lyl, c.yil - q.w);
+  } else {
+    dy = dyh + (c.yil - q.w);
+  }
+  return fmaf(dx, dx, dy * dy);
+}
+
+// The LJ pair term of li_force_kernel (src/md_cuda_common.cu:193-254) for one
+// candidate j: strict cutoff 0 < r^2 < rc_ij^2 in FP32, FP32 pair force, Kahan
+// FP32 accumulation. ENERGY adds 1/2 (u_ij - V_c) in FP64 (:795-807); VIRIAL
+// adds 1/2 r.F (:676-686) as the compensated FP32 sum of tmp*r^2.
+template <bool PY, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float& fxs, float& fxc,
+                                         float& fys, float& fyc, float& ws, float& wc,
+                                         double& u) {
+  float dx, dy;
+  const float r2 = pair_r2<PY>(q, c, dx, dy);
+  const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
+  const bool same = (tj == c.ts);
+  const float rc2 = same ? c.rc2s : c.rc2ab;
+  if (r2 < rc2 && r2 > 0.0f) {
+    const float sig2 = same ? c.sig2s : c.sig2ab;
+    const float e24 = same ? c.e24s : c.e24ab;
+    const float r2i = __frcp_rn(r2);
+    const float sr2 = sig2 * r2i;
+    const float sr6 = sr2 * sr2 * sr2;
+    const float sr12 = sr6 * sr6;
+    const float tmp = e24 * fmaf(2.0f, sr12, -sr6) * r2i;
+    kahan(fxs, fxc, tmp * dx);
+    kahan(fys, fyc, tmp * dy);
+    if (VIRIAL) kahan(ws, wc, tmp * r2);
+    if (ENERGY) {
+      const float e4 = same ? c.e4s : c.e4ab;
+      const double vc = same ? c.Vcs : c.Vcab;
+      u = fma(0.5, (double)(e4 * (sr12 - sr6)) - vc, u);
+    }
+  }
+}
+
+// Neighbour-list candidates of slot i (entry k at nlist[k * ntot + i]).
+template <bool PY, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
+                                          const int32_t* __restrict__ nlist, int64_t ntot,
+                                          int64_t i, int nn, const PairCtx& c, float& fxs,
+                                          float& fxc, float& fys, float& fyc, float& ws,
+                                          float& wc, double& u) {
+  const int32_t* __restrict__ p = nlist + i;
+#pragma unroll 4
+  for (int k = 0; k < nn; ++k) {
+    const int j = __ldg(p + (int64_t)k * ntot);
+    pair_one<PY, ENERGY, VIRIAL>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u);
+  }
+}
+
+// Candidates j in [j0, j1) (cell stencil rows or the whole system).
 template <bool PY, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
                                            const PairCtx& c, float& fxs, float& fxc, float& fys,
                                            float& fyc, float& ws, float& wc, double& u) {
 #pragma unroll 4
-  for (int j = j0; j < j1; ++j) {
-    const float4 q = __ldg(pff + j);
-    float dxh = c.xih - fabsf(q.x);
-    const float sx = rintf(dxh * c.invLx);
-    dxh = fmaf(-sx, c.Lxh, dxh);
-    const float dx = dxh + fmaf(-sx, c.Lxl, c.xil - q.z);
-    float dyh = c.yih - fabsf(q.y);
-    float dy;
-    if (PY) {
-      const float sy = rintf(dyh * c.invLy);
-      dyh = fmaf(-sy, c.Lyh, dyh);
-      dy = dyh + fmaf(-sy, c.Lyl, c.yil - q.w);
-    } else {
-      dy = dyh + (c.yil - q.w);
-    }
-    const float r2 = fmaf(dx, dx, dy * dy);
-    const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
-    const bool same = (tj == c.ts);
-    const float rc2 = same ? c.rc2s : c.rc2ab;
-    if (r2 < rc2 && r2 > 0.0f) {
-      const float sig2 = same ? c.sig2s : c.sig2ab;
-      const float e24 = same ? c.e24s : c.e24ab;
-      const float r2i = __frcp_rn(r2);
-      const float sr2 = sig2 * r2i;
-      const float sr6 = sr2 * sr2 * sr2;
-      const float sr12 = sr6 * sr6;
-      const float tmp = e24 * fmaf(2.0f, sr12, -sr6) * r2i;
-      kahan(fxs, fxc, tmp * dx);
-      kahan(fys, fyc, tmp * dy);
-      if (VIRIAL) kahan(ws, wc, tmp * r2);
-      if (ENERGY) {
-        const float e4 = same ? c.e4s : c.e4ab;
-        const double vc = same ? c.Vcs : c.Vcab;
-        u = fma(0.5, (double)(e4 * (sr12 - sr6)) - vc, u);
-      }
-    }
-  }
+  for (int j = j0; j < j1; ++j) pair_one<PY, ENERGY, VIRIAL>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u);
 }
 
 __device__ __forceinline__ void split_box(double L, float& h, float& l, float& inv) {
@@ -277,7 +304,10 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   float fxs = 0.f, fxc = 0.f, fys = 0.f, fyc = 0.f, ws = 0.f, wc = 0.f;
   u = 0.0;
   const float4* __restrict__ pff = D.pff;
-  if (S.allpairs) {
+  const int nn = __ldg(D.ncount + i);
+  if (nn >= 0) {
+    pair_list<PY, ENERGY, VIRIAL>(pff, D.nlist, D.ntot, i, nn, c, fxs, fxc, fys, fyc, ws, wc, u);
+  } else if (S.allpairs) {
     pair_range<PY, ENERGY, VIRIAL>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
                                    wc, u);
   } else {
@@ -345,15 +375,13 @@ __device__ __forceinline__ double wall_terms(double y, double Ly, double k, doub
 // y image convention (false = the piston's walled y axis, which also applies
 // the soft walls in FM_INIT/FM_OBS).
 template <int FM, bool PY>
-__global__ void __launch_bounds__(kThreads) k_force(Dev D) {
+__global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   const int b = blockIdx.x;
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
   const bool skip = (S->done != 0) || (S->err != 0) ||
                     (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
-  const int64_t i = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
-  const bool act = !skip && (i < P.p0 + P.n);
   constexpr bool kEnergy = (FM == FM_OBS);
   constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
   double red[kNP];
@@ -363,21 +391,29 @@ __global__ void __launch_bounds__(kThreads) k_force(Dev D) {
   int bad = 0;
   const double Lx = S->Lx, Ly = S->Ly;
   const double dt = P.dt, h = 0.5 * dt;
-  if (act) {
+  const int items = P.items;
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * items + threadIdx.x;
+  const int64_t end = P.p0 + P.n;
+  const double xi2 = (FM == FM_NH) ? S->xi : 0.0;
+  const double fdt = (FM == FM_FIRE) ? S->f_dt : 0.0;
+#pragma unroll 1
+  for (int it = 0; it < items; ++it) {
+    const int64_t i = base + (int64_t)it * kThreads;
+    if (skip || i >= end) break;
     const int ti = D.type[i];
     double fx, fy, w, u;
     particle_force<PY, kEnergy, kVirial>(D, P, *S, i, ti, Lx, Ly, fx, fy, w, u);
     const double m = type_mass(P, ti);
     double2 v = D.vel[i];
     if (FM == FM_OBS) {
-      red[0] = u;
-      red[1] = w;
-      red[2] = m * fma(v.x, v.x, v.y * v.y);
+      red[0] += u;
+      red[1] += w;
+      red[2] += m * fma(v.x, v.x, v.y * v.y);
       if (!PY) {
         double up, en;
         wall_terms(D.pos[i].y, Ly, P.k_piston, up, en);
-        red[3] = up;
-        red[4] = en;
+        red[3] += up;
+        red[4] += en;
       }
     } else {
       double ax = fx / m, ay = fy / m;
@@ -385,25 +421,23 @@ __global__ void __launch_bounds__(kThreads) k_force(Dev D) {
         double up, en;
         const double wf = wall_terms(D.pos[i].y, Ly, P.k_piston, up, en);
         if (wf != 0.0) ay = ay + wf / m;
-        red[0] = up;
-        red[1] = en;
+        red[0] += up;
+        red[1] += en;
       }
       if (FM == FM_NVE || FM == FM_PISTON) {
         v.x = fma(h, ax, v.x);
         v.y = fma(h, ay, v.y);
       } else if (FM == FM_NH) {
-        const double xi2 = S->xi;
         v.x = fma(h, fma(-xi2, v.x, ax), v.x);
         v.y = fma(h, fma(-xi2, v.y, ay), v.y);
-        red[0] = (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+        red[0] += (0.5 * m) * fma(v.x, v.x, v.y * v.y);
       } else if (FM == FM_NPH) {
-        red[0] = m * fma(v.x, v.x, v.y * v.y);
+        red[0] += m * fma(v.x, v.x, v.y * v.y);
         v.x = fma(h, ax, v.x);
         v.y = fma(h, ay, v.y);
-        red[1] = m * fma(v.x, v.x, v.y * v.y);
-        red[2] = w;
+        red[1] += m * fma(v.x, v.x, v.y * v.y);
+        red[2] += w;
       } else if (FM == FM_FIRE) {
-        const double fdt = S->f_dt;
         v.x = fma(fdt, ax, v.x);
         v.y = fma(fdt, ay, v.y);
         // ForceMag / PowerVal of reduce_force_metrics (src/md_energy_minimizer.cu:416-446)
@@ -411,9 +445,9 @@ __global__ void __launch_bounds__(kThreads) k_force(Dev D) {
         if (fm != fm) {
           mx[1] = 1.0;  // NaN |a|: never converged
         } else {
-          mx[0] = fm;
+          mx[0] = fmax(mx[0], fm);
         }
-        red[0] = fma(v.x, ax, v.y * ay);
+        red[0] += fma(v.x, ax, v.y * ay);
       }
       D.acc[i] = make_double2(ax, ay);
       if (FM != FM_INIT) D.vel[i] = v;
@@ -509,7 +543,6 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
   const bool skip = (S->done != 0) || (S->err != 0) || (DMd == DM_FIRE && S->f_drift == 0);
-  const int64_t i = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
   const double dt = P.dt, h = 0.5 * dt;
   const double Lx_old = S->Lx, Ly_old = S->Ly;
   double Lx = Lx_old, Ly = Ly_old;
@@ -568,13 +601,20 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
     alpha = S->f_alpha;
     zero_v = S->f_zero_v;
   }
-  const bool act = !skip && !boxbad && (i < P.p0 + P.n);
   double red[kNP];
 #pragma unroll
   for (int k = 0; k < kNP; ++k) red[k] = 0.0;
   double mx[3] = {0.0, 0.0, 0.0};
   int bad = 0;
-  if (act) {
+  const double ilx = 1.0 / Lx, ily = 1.0 / Ly;
+  const double ilx_old = 1.0 / Lx_old, ily_old = 1.0 / Ly_old;
+  const int items = P.items;
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * items + threadIdx.x;
+  const int64_t end = P.p0 + P.n;
+#pragma unroll 1
+  for (int it = 0; it < items; ++it) {
+    const int64_t i = base + (int64_t)it * kThreads;
+    if (skip || boxbad || i >= end) break;
     double2 x = D.pos[i];
     double2 v = D.vel[i];
     const double2 a = D.acc[i];
@@ -593,7 +633,7 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
       v.y = fma(h, fma(-xi1, v.y, a.y), v.y);
       x.x = fma(dt, v.x, x.x);
       x.y = fma(dt, v.y, x.y);
-      red[0] = (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+      red[0] += (0.5 * m) * fma(v.x, v.x, v.y * v.y);
     } else if (DMd == DM_NPH) {
       // step_half_nph_velocity_kernel + step_nph_scale_and_drift_kernel (:411-440)
       v.x = fma(h, a.x, v.x);
@@ -626,7 +666,6 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
     D.vel[i] = v;
     D.pff[i] = encode_ff(x.x, x.y, t, P.offx, P.offy);
     // displacement since the last rebuild and the single-step jump
-    const double ilx = 1.0 / Lx, ily = 1.0 / Ly;
     const float2 sb = D.sb[i];
     float dsx = (float)(x.x * ilx) - sb.x;
     dsx -= rintf(dsx);
@@ -639,11 +678,11 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
     } else {
       dyr = fabs(x.y - (double)sb.y);
     }
-    const double jx = fabs(xu * ilx - x0.x * (1.0 / Lx_old)) * Lx;
-    const double jy = (DMd == DM_PISTON) ? fabs(yu - x0.y) : fabs(yu * ily - x0.y * (1.0 / Ly_old)) * Ly;
-    mx[0] = dxr;
-    mx[1] = dyr;
-    mx[2] = fmax(jx, jy);
+    const double jx = fabs(xu * ilx - x0.x * ilx_old) * Lx;
+    const double jy = (DMd == DM_PISTON) ? fabs(yu - x0.y) : fabs(yu * ily - x0.y * ily_old) * Ly;
+    mx[0] = fmax(mx[0], dxr);
+    mx[1] = fmax(mx[1], dyr);
+    mx[2] = fmax(mx[2], fmax(jx, jy));
     if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(v.x) || !isfinite(v.y)) {
       bad = 1;
       mx[2] = __longlong_as_double(0x7ff0000000000000ULL);
@@ -673,16 +712,24 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
         S->Ly = Ly;
         S->clamped = clamped;
       }
-      // rebuild criterion: a pair inside the cutoff now was within one cell
-      // width (per axis) at the last rebuild while 2*max displacement +
-      // rc_max stays below the current cell width.
+      // Rebuild criterion. Cell stencil: a pair inside the cutoff now was
+      // within one cell width (per axis) at the last rebuild while
+      // 2*max displacement + rc_max stays below the current cell width.
+      // Neighbour lists (radius rc_ij + skin at the last rebuild): with the
+      // box scaled by f since then, a pair outside the list is still outside
+      // rc while 2*max displacement < f*skin - max(0, 1-f)*rc_max.
       const double slop = 1e-3 + 4e-7 * fmax(Lx, Ly);
       const double wx = Lx / (double)S->ncx;
       const double wy = (DMd == DM_PISTON) ? (S->Ly_b / (double)S->ncy) : Ly / (double)S->ncy;
+      const double fx = Lx / S->Lx_b;
+      const double fy = (DMd == DM_PISTON) ? 1.0 : Ly / S->Ly_b;
+      const double f = fmin(fx, fy);
+      const double dmax = sqrt(tmx[0] * tmx[0] + tmx[1] * tmx[1]);
       int need = 0;
       if (!S->allpairs) {
         if (2.0 * tmx[0] + slop + P.rc_max >= wx) need = 1;
         if (2.0 * tmx[1] + slop + P.rc_max >= wy) need = 1;
+        if (2.0 * dmax + slop >= f * P.skin - fmax(0.0, 1.0 - f) * P.rc_max) need = 1;
         if (!(tmx[2] <= P.skin)) need = 1;  // large single-step moves, NaN
       } else {
         need = (!(tmx[2] <= 0.25 * fmin(Lx, Ly))) ? 1 : 0;
@@ -704,15 +751,17 @@ __global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
-  const int64_t i = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
   double red[kNP];
 #pragma unroll
   for (int k = 0; k < kNP; ++k) red[k] = 0.0;
   double mx[3] = {0.0, 0.0, 0.0};
-  if (i < P.p0 + P.n) {
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * P.items + threadIdx.x;
+  for (int it = 0; it < P.items; ++it) {
+    const int64_t i = base + (int64_t)it * kThreads;
+    if (i >= P.p0 + P.n) break;
     const double2 v = D.vel[i];
     const double m = type_mass(P, D.type[i]);
-    red[0] = (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+    red[0] += (0.5 * m) * fma(v.x, v.x, v.y * v.y);
   }
   block_reduce(red, mx);
   if (!publish_last(D, S, P.nb, red, mx)) return;
@@ -773,6 +822,7 @@ __global__ void k_rb_zero(Dev D) {
     S->inv_wy = (double)ncy / Ly;
     S->Lx_b = Lx;
     S->Ly_b = Ly;
+    S->nl_overflow = 0;
   }
 }
 
@@ -951,6 +1001,95 @@ __global__ void k_rb_copyback(Dev D) {
     D.type[k] = D.type2[k];
     D.theta[k] = D.theta2[k];
     D.orig[k] = D.orig2[k];
+  }
+}
+
+// Verlet list of one slot: the 3x3 stencil candidates within the list radius
+// (rc_ij + skin), same displacement arithmetic as the force loop.
+template <bool PY>
+__device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, const SysState& S,
+                                          int64_t k) {
+  PairCtx c;
+  const float4 qi = D.pff[k];
+  c.xih = fabsf(qi.x);
+  c.yih = fabsf(qi.y);
+  c.xil = qi.z;
+  c.yil = qi.w;
+  split_box(S.Lx, c.Lxh, c.Lxl, c.invLx);
+  split_box(S.Ly, c.Lyh, c.Lyl, c.invLy);
+  const uint32_t tci =
+      (__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u);
+  const uint32_t ts = (tci == 2u) ? 99u : tci;
+  const float rl2s = P.frl2[tci == 2u ? 2 : tci], rl2ab = P.frl2[2];
+  const int ncx = S.ncx, ncy = S.ncy;
+  const int cell = D.cell_of[k];
+  const int cx = cell % ncx, cy = cell / ncx;
+  int cnt = 0;
+  const int maxn = D.max_nbr;
+  for (int dr = -1; dr <= 1; ++dr) {
+    int yy = cy + dr;
+    if (PY) {
+      if (yy < 0) yy += ncy;
+      if (yy >= ncy) yy -= ncy;
+    } else if (yy < 0 || yy >= ncy) {
+      continue;
+    }
+    const int64_t row = P.c0 + (int64_t)yy * ncx;
+    int r0[2], r1[2], nr;
+    if (cx > 0 && cx < ncx - 1) {
+      r0[0] = D.cstart[row + cx - 1];
+      r1[0] = D.cstart[row + cx + 2];
+      nr = 1;
+    } else if (cx == 0) {
+      r0[0] = D.cstart[row];
+      r1[0] = D.cstart[row + 2];
+      r0[1] = D.cstart[row + ncx - 1];
+      r1[1] = D.cstart[row + ncx];
+      nr = 2;
+    } else {
+      r0[0] = D.cstart[row + ncx - 2];
+      r1[0] = D.cstart[row + ncx];
+      r0[1] = D.cstart[row];
+      r1[1] = D.cstart[row + 1];
+      nr = 2;
+    }
+    for (int r = 0; r < nr; ++r) {
+      for (int j = r0[r]; j < r1[r]; ++j) {
+        if (j == k) continue;
+        const float4 q = D.pff[j];
+        float dx, dy;
+        const float r2 = pair_r2<PY>(q, c, dx, dy);
+        const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
+        const float rl2 = (tj == ts) ? rl2s : rl2ab;
+        if (r2 < rl2) {
+          if (cnt < maxn) D.nlist[(int64_t)cnt * D.ntot + k] = j;
+          ++cnt;
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+__global__ void k_rb_nlist(Dev D) {
+  if (!rebuild_requested(D)) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < D.ntot; k += stride) {
+    const int s = D.sysid[k];
+    if (!sys_rebuilds(D, s)) continue;
+    const SysParams& P = D.sp[s];
+    SysState* S = D.st + s;
+    if (S->allpairs || D.max_nbr <= 0) {
+      D.ncount[k] = -1;
+      continue;
+    }
+    const int cnt = S->periodic_y ? build_list<true>(D, P, *S, k) : build_list<false>(D, P, *S, k);
+    if (cnt > D.max_nbr) {
+      D.ncount[k] = -1;  // too many neighbours: the force loop scans the stencil
+      atomicAdd(&S->nl_overflow, 1);
+    } else {
+      D.ncount[k] = cnt;
+    }
   }
 }
 
