@@ -254,7 +254,20 @@ int Engine::build() {
   MDB_ALLOC(D.perm, ntot_);
   D.max_nbr = max_nbr_;
   MDB_ALLOC(D.ncount, ntot_);
-  if (max_nbr_ > 0) MDB_ALLOC(D.nlist, (int64_t)max_nbr_ * ntot_);
+  // 16-bit list offsets when the stencil of every system spans well under
+  // 32768 slots (about two cell rows); a particle whose offsets still do not
+  // fit falls back to scanning its stencil.
+  D.nl16 = 1;
+  for (int s = 0; s < ns; ++s) {
+    const double rows = std::max(1.0, floor(hsp_[s].Ly0 / hsp_[s].r_cell));
+    if (3.0 * hsp_[s].n / rows >= 30000.0) D.nl16 = 0;
+  }
+  if (max_nbr_ > 0) {
+    if (D.nl16)
+      MDB_ALLOC(D.nlist16, (int64_t)max_nbr_ * ntot_);
+    else
+      MDB_ALLOC(D.nlist, (int64_t)max_nbr_ * ntot_);
+  }
   MDB_ALLOC(D.ccount, ncells_);
   MDB_ALLOC(D.ccursor, ncells_);
   MDB_ALLOC(D.cstart, ncells_ + 1);

@@ -118,9 +118,11 @@ struct Dev {
   int32_t* cell_of;
   int32_t* key;
   int32_t* perm;
-  int32_t* nlist;     // neighbour list, entry k of slot i at nlist[k * ntot + i]
+  int32_t* nlist;     // neighbour list, offset j - i of entry k of slot i at
+  int16_t* nlist16;   //   nlist[k * ntot + i] (int32) or nlist16[...] (int16)
   int32_t* ncount;    // list length per slot, -1: use the cell stencil
   int32_t max_nbr;
+  int32_t nl16;       // 1: 16-bit offsets (every stencil offset fits in int16)
   int32_t* ccount;
   int32_t* ccursor;
   int32_t* cstart;    // ncells + 1

@@ -16,12 +16,25 @@ namespace mdb {
 
 // ---------------------------------------------------------------- helpers --
 
-// pbc_wrap_hd (include/md_cuda_common.hpp:20-29).
+// pbc_wrap_hd (include/md_cuda_common.hpp:20-29): fmod(x, L), then + L when
+// negative. For -L <= x < 2L the branches below give the same bits as fmod
+// (x - L is exact there), which covers every step but pathological jumps.
 __device__ __forceinline__ double pbc_wrap(double x, double L) {
   if (L <= 0.0) return x;
+  if (x >= 0.0 && x < L) return x;
+  if (x >= L && x < 2.0 * L) return x - L;
+  if (x < 0.0 && x >= -L) return x + L;
   x = fmod(x, L);
   if (x < 0.0) x += L;
   return x;
+}
+
+// 1/x from the hardware approximation refined by one Newton-Raphson step
+// (r1 = r0 + r0 (1 - x r0)); within one ulp of the IEEE quotient.
+__device__ __forceinline__ float recip(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return fmaf(r, fmaf(-x, r, 1.0f), r);
 }
 
 // Type class for the parameter table (src/md_cuda_common.cu:218-229):
@@ -228,7 +241,7 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
   if (r2 < rc2 && r2 > 0.0f) {
     const float sig2 = same ? c.sig2s : c.sig2ab;
     const float e24 = same ? c.e24s : c.e24ab;
-    const float r2i = __frcp_rn(r2);
+    const float r2i = recip(r2);
     const float sr2 = sig2 * r2i;
     const float sr6 = sr2 * sr2 * sr2;
     const float sr12 = sr6 * sr6;
@@ -244,18 +257,40 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
   }
 }
 
-// Neighbour-list candidates of slot i (entry k at nlist[k * ntot + i]).
-template <bool PY, bool ENERGY, bool VIRIAL>
+// Neighbour-list candidates of slot i. Entry k holds the offset d of the
+// partner j from i inside the system's slot range, taken modulo the system
+// size n into [-n/2, n/2) (so the stencil rows across the periodic y edge stay
+// small): int16 at nlist16[k * ntot + i] when the batch uses 16-bit offsets,
+// else int32 at nlist[k * ntot + i]. Offsets are fetched eight at a time
+// before the dependent position gathers to keep several loads in flight.
+template <bool PY, bool ENERGY, bool VIRIAL, typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
-                                          const int32_t* __restrict__ nlist, int64_t ntot,
-                                          int64_t i, int nn, const PairCtx& c, float& fxs,
+                                          const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
+                                          int li, int n, int nn, const PairCtx& c, float& fxs,
                                           float& fxc, float& fys, float& fyc, float& ws,
                                           float& wc, double& u) {
-  const int32_t* __restrict__ p = nlist + i;
-#pragma unroll 4
-  for (int k = 0; k < nn; ++k) {
-    const int j = __ldg(p + (int64_t)k * ntot);
-    pair_one<PY, ENERGY, VIRIAL>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u);
+  const IDX* __restrict__ p = nlist + i;
+  const float4* __restrict__ base = pff + (i - li);  // slot 0 of the system
+  constexpr int PF = (ENERGY || VIRIAL) ? 4 : 8;  // prefetch width (register budget)
+  int k = 0;
+  for (; k + PF <= nn; k += PF) {
+    int j[PF];
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+      int t = li + (int)__ldg(p + (int64_t)(k + q) * ntot);
+      t += (t < 0) ? n : 0;
+      t -= (t >= n) ? n : 0;
+      j[q] = t;
+    }
+#pragma unroll
+    for (int q = 0; q < PF; ++q)
+      pair_one<PY, ENERGY, VIRIAL>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u);
+  }
+  for (; k < nn; ++k) {
+    int t = li + (int)__ldg(p + (int64_t)k * ntot);
+    t += (t < 0) ? n : 0;
+    t -= (t >= n) ? n : 0;
+    pair_one<PY, ENERGY, VIRIAL>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u);
   }
 }
 
@@ -306,7 +341,13 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   const float4* __restrict__ pff = D.pff;
   const int nn = __ldg(D.ncount + i);
   if (nn >= 0) {
-    pair_list<PY, ENERGY, VIRIAL>(pff, D.nlist, D.ntot, i, nn, c, fxs, fxc, fys, fyc, ws, wc, u);
+    const int li = (int)(i - P.p0);
+    if (D.nl16)
+      pair_list<PY, ENERGY, VIRIAL>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc, fys,
+                                    fyc, ws, wc, u);
+    else
+      pair_list<PY, ENERGY, VIRIAL>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc, fys, fyc,
+                                    ws, wc, u);
   } else if (S.allpairs) {
     pair_range<PY, ENERGY, VIRIAL>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
                                    wc, u);
@@ -1026,6 +1067,7 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
   const int cx = cell % ncx, cy = cell / ncx;
   int cnt = 0;
   const int maxn = D.max_nbr;
+  const int half = (P.n + 1) / 2;
   for (int dr = -1; dr <= 1; ++dr) {
     int yy = cy + dr;
     if (PY) {
@@ -1062,7 +1104,16 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
         const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
         const float rl2 = (tj == ts) ? rl2s : rl2ab;
         if (r2 < rl2) {
-          if (cnt < maxn) D.nlist[(int64_t)cnt * D.ntot + k] = j;
+          int d = j - (int)k;  // offset modulo n into [-n/2, n/2)
+          if (d >= half) d -= P.n;
+          if (d < -half) d += P.n;
+          if (D.nl16 && (d > 32767 || d < -32768)) return maxn + 1;  // use the stencil
+          if (cnt < maxn) {
+            if (D.nl16)
+              D.nlist16[(int64_t)cnt * D.ntot + k] = (int16_t)d;
+            else
+              D.nlist[(int64_t)cnt * D.ntot + k] = d;
+          }
           ++cnt;
         }
       }
