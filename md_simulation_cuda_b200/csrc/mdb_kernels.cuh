@@ -130,44 +130,78 @@ __device__ __forceinline__ void block_reduce(double (&s)[kNP], double (&m)[3]) {
   __syncthreads();
 }
 
-// Publishes this block's partials (thread 0 holds them) and tells every
-// thread of the block whether it is the last of its system to finish.
-__device__ __forceinline__ bool publish_last(const Dev& D, SysState* S, int nb,
-                                             const double (&s)[kNP], const double (&m)[3]) {
-  __shared__ int am_last;
+// Sums (and maxima) of one value set over the blocks of a system, without a
+// second launch and independent of block timing: each block publishes its
+// partials; the last block of every group of kGroup blocks sums that group in
+// a fixed order; the last group to finish sums the group partials in a fixed
+// order. Returns true in that final block, whose thread 0 then holds the
+// system totals in tot/tmx. red/mx hold the calling thread's contributions.
+__device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, SysState* S,
+                                              double (&red)[kNP], double (&mx)[3],
+                                              double (&tot)[kNP], double (&tmx)[3]) {
+  __shared__ int sh_last_group, sh_last_system;
+  block_reduce(red, mx);
+  const int lb = (int)blockIdx.x - P.b0;
+  const int g = lb / kGroup;
+  const int gsize = min(kGroup, P.nb - g * kGroup);
+  const int ng = (P.nb + kGroup - 1) / kGroup;
+  const int gg = P.g0 + g;
   if (threadIdx.x == 0) {
     double* p = D.part + (size_t)blockIdx.x * kNP;
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) p[k] = s[k];
+    for (int k = 0; k < kNP; ++k) p[k] = red[k];
     double* pm = D.partm + (size_t)blockIdx.x * 4;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) pm[k] = m[k];
+    for (int k = 0; k < 3; ++k) pm[k] = mx[k];
     __threadfence();
-    const unsigned prev = atomicAdd(&S->counter, 1u);
-    am_last = (prev == (unsigned)(nb - 1)) ? 1 : 0;
+    const unsigned prev = atomicAdd(D.gcount + gg, 1u);
+    sh_last_group = (prev == (unsigned)(gsize - 1)) ? 1 : 0;
   }
   __syncthreads();
-  const bool last = am_last != 0;
-  if (last) __threadfence();
-  return last;
-}
-
-// Deterministic totals over the system's blocks (strided, then fixed tree).
-__device__ __forceinline__ void system_totals(const Dev& D, int b0, int nb, double (&s)[kNP],
-                                              double (&m)[3]) {
+  if (!sh_last_group) return false;
+  __threadfence();
+  double s[kNP];
+  double m[3];
 #pragma unroll
   for (int k = 0; k < kNP; ++k) s[k] = 0.0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) m[k] = 0.0;
-  for (int b = threadIdx.x; b < nb; b += kThreads) {
-    const double* p = D.part + (size_t)(b0 + b) * kNP;
-    const double* pm = D.partm + (size_t)(b0 + b) * 4;
+  if ((int)threadIdx.x < gsize) {
+    const size_t blk = (size_t)(P.b0 + g * kGroup + threadIdx.x);
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) s[k] += __ldcg(p + k);
+    for (int k = 0; k < kNP; ++k) s[k] = __ldcg(D.part + blk * kNP + k);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) m[k] = fmax(m[k], __ldcg(pm + k));
+    for (int k = 0; k < 3; ++k) m[k] = __ldcg(D.partm + blk * 4 + k);
   }
   block_reduce(s, m);
+  if (threadIdx.x == 0) {
+    double* p = D.gpart + (size_t)gg * kNP;
+#pragma unroll
+    for (int k = 0; k < kNP; ++k) p[k] = s[k];
+    double* pm = D.gpartm + (size_t)gg * 4;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) pm[k] = m[k];
+    D.gcount[gg] = 0u;
+    __threadfence();
+    const unsigned prev = atomicAdd(&S->counter, 1u);
+    sh_last_system = (prev == (unsigned)(ng - 1)) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!sh_last_system) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < kNP; ++k) tot[k] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) tmx[k] = 0.0;
+  for (int q = threadIdx.x; q < ng; q += kThreads) {
+    const size_t gq = (size_t)(P.g0 + q);
+#pragma unroll
+    for (int k = 0; k < kNP; ++k) tot[k] += __ldcg(D.gpart + gq * kNP + k);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) tmx[k] = fmax(tmx[k], __ldcg(D.gpartm + gq * 4 + k));
+  }
+  block_reduce(tot, tmx);
+  return true;
 }
 
 // Counts finished systems; the last one sets the graph condition for the
@@ -208,9 +242,16 @@ struct PairCtx {
 // Displacement i - j with the nearest image: the hi parts of two coordinates
 // in the same binade subtract exactly, the image shift s*L_hi is exact, the lo
 // parts carry the remaining bits, one rounding at the end.
-template <bool PY>
+// MIC = false: both particles are known to sit on the same side of every
+// periodic edge (no image shift needed).
+template <bool PY, bool MIC = true>
 __device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float& dx, float& dy) {
   float dxh = c.xih - fabsf(q.x);
+  if (!MIC) {
+    dx = dxh + (c.xil - q.z);
+    dy = (c.yih - fabsf(q.y)) + (c.yil - q.w);
+    return fmaf(dx, dx, dy * dy);
+  }
   const float sx = rintf(dxh * c.invLx);
   dxh = fmaf(-sx, c.Lxh, dxh);
   dx = dxh + fmaf(-sx, c.Lxl, c.xil - q.z);
@@ -229,12 +270,12 @@ __device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float
 // candidate j: strict cutoff 0 < r^2 < rc_ij^2 in FP32, FP32 pair force, Kahan
 // FP32 accumulation. ENERGY adds 1/2 (u_ij - V_c) in FP64 (:795-807); VIRIAL
 // adds 1/2 r.F (:676-686) as the compensated FP32 sum of tmp*r^2.
-template <bool PY, bool ENERGY, bool VIRIAL>
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC = true>
 __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float& fxs, float& fxc,
                                          float& fys, float& fyc, float& ws, float& wc,
                                          double& u) {
   float dx, dy;
-  const float r2 = pair_r2<PY>(q, c, dx, dy);
+  const float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
   const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
   const bool same = (tj == c.ts);
   const float rc2 = same ? c.rc2s : c.rc2ab;
@@ -263,7 +304,7 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
 // small): int16 at nlist16[k * ntot + i] when the batch uses 16-bit offsets,
 // else int32 at nlist[k * ntot + i]. Offsets are fetched eight at a time
 // before the dependent position gathers to keep several loads in flight.
-template <bool PY, bool ENERGY, bool VIRIAL, typename IDX>
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
                                           int li, int n, int nn, const PairCtx& c, float& fxs,
@@ -284,13 +325,13 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
     }
 #pragma unroll
     for (int q = 0; q < PF; ++q)
-      pair_one<PY, ENERGY, VIRIAL>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u);
+      pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u);
   }
   for (; k < nn; ++k) {
     int t = li + (int)__ldg(p + (int64_t)k * ntot);
     t += (t < 0) ? n : 0;
     t -= (t >= n) ? n : 0;
-    pair_one<PY, ENERGY, VIRIAL>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u);
+    pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u);
   }
 }
 
@@ -342,12 +383,27 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   const int nn = __ldg(D.ncount + i);
   if (nn >= 0) {
     const int li = (int)(i - P.p0);
-    if (D.nl16)
-      pair_list<PY, ENERGY, VIRIAL>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc, fys,
-                                    fyc, ws, wc, u);
-    else
-      pair_list<PY, ENERGY, VIRIAL>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc, fys, fyc,
-                                    ws, wc, u);
+    // Interior build cells (two or more cells from each periodic edge): the
+    // list partners were binned one cell away at most and move less than
+    // half a cell before the next rebuild, so no pair straddles an edge.
+    const int cell = __ldg(D.cell_of + i);
+    const int cx = cell % S.ncx, cy = cell / S.ncx;
+    const bool interior = cx >= 2 && cx <= S.ncx - 3 && (!PY || (cy >= 2 && cy <= S.ncy - 3));
+    if (D.nl16) {
+      if (interior)
+        pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+                                             fys, fyc, ws, wc, u);
+      else
+        pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+                                            fys, fyc, ws, wc, u);
+    } else {
+      if (interior)
+        pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+                                             fys, fyc, ws, wc, u);
+      else
+        pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+                                            fys, fyc, ws, wc, u);
+    }
   } else if (S.allpairs) {
     pair_range<PY, ENERGY, VIRIAL>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
                                    wc, u);
@@ -496,11 +552,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
     }
   }
   if (bad) atomicOr(&S->nonfinite, 1);
-  block_reduce(red, mx);
-  if (!publish_last(D, S, P.nb, red, mx)) return;
   double tot[kNP];
   double tmx[3];
-  system_totals(D, P.b0, P.nb, tot, tmx);
+  if (!reduce_system(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   if (!skip) {
     if (FM == FM_NH) {
@@ -578,7 +632,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
 // float-float refresh, displacement since the last rebuild. The system's last
 // block applies the scalar updates and the rebuild criterion.
 template <int DMd>
-__global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
+__global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   const int b = blockIdx.x;
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
@@ -730,11 +784,9 @@ __global__ void __launch_bounds__(kThreads) k_drift(Dev D) {
     }
   }
   if (bad) atomicOr(&S->nonfinite, 1);
-  block_reduce(red, mx);
-  if (!publish_last(D, S, P.nb, red, mx)) return;
   double tot[kNP];
   double tmx[3];
-  system_totals(D, P.b0, P.nb, tot, tmx);
+  if (!reduce_system(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   if (!skip) {
     if (boxbad) {
@@ -804,11 +856,9 @@ __global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
     const double m = type_mass(P, D.type[i]);
     red[0] += (0.5 * m) * fma(v.x, v.x, v.y * v.y);
   }
-  block_reduce(red, mx);
-  if (!publish_last(D, S, P.nb, red, mx)) return;
   double tot[kNP];
   double tmx[3];
-  system_totals(D, P.b0, P.nb, tot, tmx);
+  if (!reduce_system(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   S->K = tot[0];
   S->counter = 0u;

@@ -110,8 +110,9 @@ def test_two_particle_analytic(built):
             pos = np.array([[x0, 5.0], [(x0 + r) % L, 5.0]])
             acc, U, W = mdb.compute_forces(cfg, _frame(pos, [0, 0]), L, L)
             F = 24 * (2 * r ** -13 - r ** -7)
-            assert abs(acc[0, 0] + F) <= 1e-6 * abs(F) + 1e-6
-            assert abs(acc[1, 0] - F) <= 1e-6 * abs(F) + 1e-6
+            # FP32 pair term; near the minimum 2 sr^12 - sr^6 cancels ~8x
+            assert abs(acc[0, 0] + F) <= 1e-5 * abs(F) + 1e-6
+            assert abs(acc[1, 0] - F) <= 1e-5 * abs(F) + 1e-6
             U0 = 4 * (r ** -12 - r ** -6) - Vc
             assert abs(U - U0) <= 1e-6 * (1.0 + abs(U0))  # FP32 pair energy
     # beyond the cutoff: nothing
