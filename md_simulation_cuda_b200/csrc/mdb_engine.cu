@@ -121,7 +121,7 @@ int Engine::build() {
   const int64_t wave = (int64_t)nsm * 4 * kThreads;
   // MDB_ITEMS=<k> fixes the particles per thread (tuning aid; 0 = automatic).
   const char* items_env = getenv("MDB_ITEMS");
-  const int items_fixed = items_env ? atoi(items_env) : 1;
+  const int items_fixed = items_env ? atoi(items_env) : 0;
   int g0 = 0;
   for (int s = 0; s < ns; ++s) {
     const SystemSpec& sp = specs_[s];

@@ -97,32 +97,34 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// Fixed-order block reduction of kNP sums and 3 maxima (non-negative
-// values); valid in thread 0. The tree depends only on blockDim, so results
-// are bit-reproducible.
+// Fixed-order block reduction of the first NS sums and NM maxima
+// (non-negative values); valid in thread 0. The tree depends only on
+// blockDim, so results are bit-reproducible.
+template <int NS, int NM>
 __device__ __forceinline__ void block_reduce(double (&s)[kNP], double (&m)[3]) {
-  __shared__ double sh_s[kNP][kThreads / 32];
-  __shared__ double sh_m[3][kThreads / 32];
+  if (NS == 0 && NM == 0) return;
+  __shared__ double sh_s[NS > 0 ? NS : 1][kThreads / 32];
+  __shared__ double sh_m[NM > 0 ? NM : 1][kThreads / 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < kNP; ++k) s[k] = warp_sum(s[k]);
+  for (int k = 0; k < NS; ++k) s[k] = warp_sum(s[k]);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) m[k] = warp_max(m[k]);
+  for (int k = 0; k < NM; ++k) m[k] = warp_max(m[k]);
   if (lane == 0) {
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) sh_s[k][w] = s[k];
+    for (int k = 0; k < NS; ++k) sh_s[k][w] = s[k];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) sh_m[k][w] = m[k];
+    for (int k = 0; k < NM; ++k) sh_m[k][w] = m[k];
   }
   __syncthreads();
   if (w == 0) {
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) {
+    for (int k = 0; k < NS; ++k) {
       double v = lane < kThreads / 32 ? sh_s[k][lane] : 0.0;
       s[k] = warp_sum(v);
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < NM; ++k) {
       double v = lane < kThreads / 32 ? sh_m[k][lane] : 0.0;
       m[k] = warp_max(v);
     }
@@ -136,11 +138,12 @@ __device__ __forceinline__ void block_reduce(double (&s)[kNP], double (&m)[3]) {
 // a fixed order; the last group to finish sums the group partials in a fixed
 // order. Returns true in that final block, whose thread 0 then holds the
 // system totals in tot/tmx. red/mx hold the calling thread's contributions.
+template <int NS, int NM>
 __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, SysState* S,
                                               double (&red)[kNP], double (&mx)[3],
                                               double (&tot)[kNP], double (&tmx)[3]) {
   __shared__ int sh_last_group, sh_last_system;
-  block_reduce(red, mx);
+  block_reduce<NS, NM>(red, mx);
   const int lb = (int)blockIdx.x - P.b0;
   const int g = lb / kGroup;
   const int gsize = min(kGroup, P.nb - g * kGroup);
@@ -149,10 +152,10 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
   if (threadIdx.x == 0) {
     double* p = D.part + (size_t)blockIdx.x * kNP;
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) p[k] = red[k];
+    for (int k = 0; k < NS; ++k) p[k] = red[k];
     double* pm = D.partm + (size_t)blockIdx.x * 4;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) pm[k] = mx[k];
+    for (int k = 0; k < NM; ++k) pm[k] = mx[k];
     __threadfence();
     const unsigned prev = atomicAdd(D.gcount + gg, 1u);
     sh_last_group = (prev == (unsigned)(gsize - 1)) ? 1 : 0;
@@ -169,18 +172,18 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
   if ((int)threadIdx.x < gsize) {
     const size_t blk = (size_t)(P.b0 + g * kGroup + threadIdx.x);
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) s[k] = __ldcg(D.part + blk * kNP + k);
+    for (int k = 0; k < NS; ++k) s[k] = __ldcg(D.part + blk * kNP + k);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) m[k] = __ldcg(D.partm + blk * 4 + k);
+    for (int k = 0; k < NM; ++k) m[k] = __ldcg(D.partm + blk * 4 + k);
   }
-  block_reduce(s, m);
+  block_reduce<NS, NM>(s, m);
   if (threadIdx.x == 0) {
     double* p = D.gpart + (size_t)gg * kNP;
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) p[k] = s[k];
+    for (int k = 0; k < NS; ++k) p[k] = s[k];
     double* pm = D.gpartm + (size_t)gg * 4;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) pm[k] = m[k];
+    for (int k = 0; k < NM; ++k) pm[k] = m[k];
     D.gcount[gg] = 0u;
     __threadfence();
     const unsigned prev = atomicAdd(&S->counter, 1u);
@@ -196,13 +199,22 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
   for (int q = threadIdx.x; q < ng; q += kThreads) {
     const size_t gq = (size_t)(P.g0 + q);
 #pragma unroll
-    for (int k = 0; k < kNP; ++k) tot[k] += __ldcg(D.gpart + gq * kNP + k);
+    for (int k = 0; k < NS; ++k) tot[k] += __ldcg(D.gpart + gq * kNP + k);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) tmx[k] = fmax(tmx[k], __ldcg(D.gpartm + gq * 4 + k));
+    for (int k = 0; k < NM; ++k) tmx[k] = fmax(tmx[k], __ldcg(D.gpartm + gq * 4 + k));
   }
-  block_reduce(tot, tmx);
+  block_reduce<NS, NM>(tot, tmx);
   return true;
 }
+
+// Number of sums / maxima each phase reduces.
+template <int FM>
+struct ForceRed {
+  static constexpr int NS = (FM == FM_OBS) ? 5 : (FM == FM_NPH) ? 3
+                          : (FM == FM_INIT || FM == FM_PISTON) ? 2
+                          : (FM == FM_NH || FM == FM_FIRE) ? 1 : 0;
+  static constexpr int NM = (FM == FM_FIRE) ? 2 : 0;
+};
 
 // Counts finished systems; the last one sets the graph condition for the
 // rebuild body from the batch-wide flag. Called by thread 0 of a system's
@@ -481,6 +493,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
                     (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
   constexpr bool kEnergy = (FM == FM_OBS);
   constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
+  constexpr int kNS = ForceRed<FM>::NS, kNM = ForceRed<FM>::NM;
   double red[kNP];
 #pragma unroll
   for (int k = 0; k < kNP; ++k) red[k] = 0.0;
@@ -554,7 +567,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   if (bad) atomicOr(&S->nonfinite, 1);
   double tot[kNP];
   double tmx[3];
-  if (!reduce_system(D, P, S, red, mx, tot, tmx)) return;
+  if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   if (!skip) {
     if (FM == FM_NH) {
@@ -638,6 +651,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
   const bool skip = (S->done != 0) || (S->err != 0) || (DMd == DM_FIRE && S->f_drift == 0);
+  constexpr int kNS = (DMd == DM_NH) ? 1 : 0, kNM = 3;
   const double dt = P.dt, h = 0.5 * dt;
   const double Lx_old = S->Lx, Ly_old = S->Ly;
   double Lx = Lx_old, Ly = Ly_old;
@@ -786,7 +800,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   if (bad) atomicOr(&S->nonfinite, 1);
   double tot[kNP];
   double tmx[3];
-  if (!reduce_system(D, P, S, red, mx, tot, tmx)) return;
+  if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   if (!skip) {
     if (boxbad) {
@@ -844,6 +858,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
+  constexpr int kNS = 1, kNM = 0;
   double red[kNP];
 #pragma unroll
   for (int k = 0; k < kNP; ++k) red[k] = 0.0;
@@ -858,7 +873,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
   }
   double tot[kNP];
   double tmx[3];
-  if (!reduce_system(D, P, S, red, mx, tot, tmx)) return;
+  if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   S->K = tot[0];
   S->counter = 0u;
