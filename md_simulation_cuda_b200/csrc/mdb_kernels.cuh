@@ -291,7 +291,8 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
   const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
   const bool same = (tj == c.ts);
   const float rc2 = same ? c.rc2s : c.rc2ab;
-  if (r2 < rc2 && r2 > 0.0f) {
+  // 0 < r2 < rc2 for the non-negative r2 (NaN fails): bits - 1 as unsigned
+  if (__float_as_uint(r2) - 1u < __float_as_uint(rc2) - 1u) {
     const float sig2 = same ? c.sig2s : c.sig2ab;
     const float e24 = same ? c.e24s : c.e24ab;
     const float r2i = recip(r2);
@@ -644,6 +645,88 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
 // First half of a step for one slot: kick + drift + wrap (mode-specific),
 // float-float refresh, displacement since the last rebuild. The system's last
 // block applies the scalar updates and the rebuild criterion.
+struct DriftCtx {
+  double dt, h, xi1, lam, vsc, fdt, alpha, Lx, Ly, ilx, ily, ilx_old, ily_old;
+  double massA, massB, offx, offy;
+  int zero_v, py;
+};
+
+// One particle's drift from its loaded state.
+template <int DMd>
+__device__ __forceinline__ void drift_particle(const Dev& D, const DriftCtx& c, int64_t i,
+                                               double2 x, double2 v, const double2 a, int t,
+                                               const float2 sb, double& ksum, double& mdx,
+                                               double& mdy, double& mjump, int& bad) {
+  const double m = t == 0 ? c.massA : c.massB;
+  const double2 x0 = x;
+  if (DMd == DM_NVE || DMd == DM_PISTON) {
+    // step_half_vv_kernel (src/md_cuda_common.cu:381-394), piston (:396-409)
+    v.x = fma(c.h, a.x, v.x);
+    v.y = fma(c.h, a.y, v.y);
+    x.x = fma(c.dt, v.x, x.x);
+    x.y = fma(c.dt, v.y, x.y);
+  } else if (DMd == DM_NH) {
+    // step_half_vv_nh_kernel (src/md_cuda_common.cu:454-478)
+    v.x = fma(c.h, fma(-c.xi1, v.x, a.x), v.x);
+    v.y = fma(c.h, fma(-c.xi1, v.y, a.y), v.y);
+    x.x = fma(c.dt, v.x, x.x);
+    x.y = fma(c.dt, v.y, x.y);
+    ksum += (0.5 * m) * fma(v.x, v.x, v.y * v.y);
+  } else if (DMd == DM_NPH) {
+    // step_half_nph_velocity_kernel + step_nph_scale_and_drift_kernel (:411-440)
+    v.x = fma(c.h, a.x, v.x);
+    v.y = fma(c.h, a.y, v.y);
+    v.x = v.x * c.vsc;
+    v.y = v.y * c.vsc;
+    x.x = fma(c.dt, v.x, c.lam * x.x);
+    x.y = fma(c.dt, v.y, c.lam * x.y);
+  } else if (DMd == DM_FIRE) {
+    // zero_velocity / fire_velocity_mix / drift (src/md_energy_minimizer.cu:32-71)
+    if (c.zero_v) {
+      v.x = 0.0;
+      v.y = 0.0;
+    } else {
+      const double vmag = sqrt(fma(v.x, v.x, v.y * v.y));
+      const double fmag = sqrt(fma(a.x, a.x, a.y * a.y));
+      if (vmag > 0.0 && fmag > 0.0) {
+        const double scale = vmag / fmag;
+        v.x = fma(c.alpha * scale, a.x, (1.0 - c.alpha) * v.x);
+        v.y = fma(c.alpha * scale, a.y, (1.0 - c.alpha) * v.y);
+      }
+    }
+    x.x = fma(c.fdt, v.x, x.x);
+    x.y = fma(c.fdt, v.y, x.y);
+  }
+  const double xu = x.x, yu = x.y;
+  x.x = pbc_wrap(x.x, c.Lx);
+  if (DMd != DM_PISTON) x.y = pbc_wrap(x.y, c.Ly);
+  D.pos[i] = x;
+  D.vel[i] = v;
+  D.pff[i] = encode_ff(x.x, x.y, t, c.offx, c.offy);
+  // displacement since the last rebuild and the single-step jump
+  float dsx = (float)(x.x * c.ilx) - sb.x;
+  dsx -= rintf(dsx);
+  const double dxr = (double)fabsf(dsx) * c.Lx;
+  double dyr;
+  if (c.py && DMd != DM_PISTON) {
+    float dsy = (float)(x.y * c.ily) - sb.y;
+    dsy -= rintf(dsy);
+    dyr = (double)fabsf(dsy) * c.Ly;
+  } else {
+    dyr = fabs(x.y - (double)sb.y);
+  }
+  // (only the NPH step rescales the box inside the step)
+  const double jx = (DMd == DM_NPH) ? fabs(xu * c.ilx - x0.x * c.ilx_old) * c.Lx : fabs(xu - x0.x);
+  const double jy = (DMd == DM_NPH) ? fabs(yu * c.ily - x0.y * c.ily_old) * c.Ly : fabs(yu - x0.y);
+  mdx = fmax(mdx, dxr);
+  mdy = fmax(mdy, dyr);
+  mjump = fmax(mjump, fmax(jx, jy));
+  if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(v.x) || !isfinite(v.y)) {
+    bad = 1;
+    mjump = __longlong_as_double(0x7ff0000000000000ULL);
+  }
+}
+
 template <int DMd>
 __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   const int b = blockIdx.x;
@@ -720,81 +803,33 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   const int items = P.items;
   const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * items + threadIdx.x;
   const int64_t end = P.p0 + P.n;
+  DriftCtx dc;
+  dc.dt = dt;
+  dc.h = h;
+  dc.xi1 = xi1;
+  dc.lam = lam;
+  dc.vsc = vsc;
+  dc.fdt = fdt;
+  dc.alpha = alpha;
+  dc.Lx = Lx;
+  dc.Ly = Ly;
+  dc.ilx = ilx;
+  dc.ily = ily;
+  dc.ilx_old = ilx_old;
+  dc.ily_old = ily_old;
+  dc.massA = P.massA;
+  dc.massB = P.massB;
+  dc.offx = P.offx;
+  dc.offy = P.offy;
+  dc.zero_v = zero_v;
+  dc.py = py ? 1 : 0;
+  if (!skip && !boxbad) {
 #pragma unroll 1
-  for (int it = 0; it < items; ++it) {
-    const int64_t i = base + (int64_t)it * kThreads;
-    if (skip || boxbad || i >= end) break;
-    double2 x = D.pos[i];
-    double2 v = D.vel[i];
-    const double2 a = D.acc[i];
-    const int t = D.type[i];
-    const double m = type_mass(P, t);
-    const double2 x0 = x;
-    if (DMd == DM_NVE || DMd == DM_PISTON) {
-      // step_half_vv_kernel (src/md_cuda_common.cu:381-394), piston (:396-409)
-      v.x = fma(h, a.x, v.x);
-      v.y = fma(h, a.y, v.y);
-      x.x = fma(dt, v.x, x.x);
-      x.y = fma(dt, v.y, x.y);
-    } else if (DMd == DM_NH) {
-      // step_half_vv_nh_kernel (src/md_cuda_common.cu:454-478)
-      v.x = fma(h, fma(-xi1, v.x, a.x), v.x);
-      v.y = fma(h, fma(-xi1, v.y, a.y), v.y);
-      x.x = fma(dt, v.x, x.x);
-      x.y = fma(dt, v.y, x.y);
-      red[0] += (0.5 * m) * fma(v.x, v.x, v.y * v.y);
-    } else if (DMd == DM_NPH) {
-      // step_half_nph_velocity_kernel + step_nph_scale_and_drift_kernel (:411-440)
-      v.x = fma(h, a.x, v.x);
-      v.y = fma(h, a.y, v.y);
-      v.x = v.x * vsc;
-      v.y = v.y * vsc;
-      x.x = fma(dt, v.x, lam * x.x);
-      x.y = fma(dt, v.y, lam * x.y);
-    } else if (DMd == DM_FIRE) {
-      // zero_velocity / fire_velocity_mix / drift (src/md_energy_minimizer.cu:32-71)
-      if (zero_v) {
-        v.x = 0.0;
-        v.y = 0.0;
-      } else {
-        const double vmag = sqrt(fma(v.x, v.x, v.y * v.y));
-        const double fmag = sqrt(fma(a.x, a.x, a.y * a.y));
-        if (vmag > 0.0 && fmag > 0.0) {
-          const double scale = vmag / fmag;
-          v.x = fma(alpha * scale, a.x, (1.0 - alpha) * v.x);
-          v.y = fma(alpha * scale, a.y, (1.0 - alpha) * v.y);
-        }
-      }
-      x.x = fma(fdt, v.x, x.x);
-      x.y = fma(fdt, v.y, x.y);
-    }
-    const double xu = x.x, yu = x.y;
-    x.x = pbc_wrap(x.x, Lx);
-    if (DMd != DM_PISTON) x.y = pbc_wrap(x.y, Ly);
-    D.pos[i] = x;
-    D.vel[i] = v;
-    D.pff[i] = encode_ff(x.x, x.y, t, P.offx, P.offy);
-    // displacement since the last rebuild and the single-step jump
-    const float2 sb = D.sb[i];
-    float dsx = (float)(x.x * ilx) - sb.x;
-    dsx -= rintf(dsx);
-    const double dxr = (double)fabsf(dsx) * Lx;
-    double dyr;
-    if (py && DMd != DM_PISTON) {
-      float dsy = (float)(x.y * ily) - sb.y;
-      dsy -= rintf(dsy);
-      dyr = (double)fabsf(dsy) * Ly;
-    } else {
-      dyr = fabs(x.y - (double)sb.y);
-    }
-    const double jx = fabs(xu * ilx - x0.x * ilx_old) * Lx;
-    const double jy = (DMd == DM_PISTON) ? fabs(yu - x0.y) : fabs(yu * ily - x0.y * ily_old) * Ly;
-    mx[0] = fmax(mx[0], dxr);
-    mx[1] = fmax(mx[1], dyr);
-    mx[2] = fmax(mx[2], fmax(jx, jy));
-    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(v.x) || !isfinite(v.y)) {
-      bad = 1;
-      mx[2] = __longlong_as_double(0x7ff0000000000000ULL);
+    for (int it = 0; it < items; ++it) {
+      const int64_t i = base + (int64_t)it * kThreads;
+      if (i >= end) break;
+      drift_particle<DMd>(D, dc, i, D.pos[i], D.vel[i], D.acc[i], D.type[i], D.sb[i], red[0],
+                          mx[0], mx[1], mx[2], bad);
     }
   }
   if (bad) atomicOr(&S->nonfinite, 1);
