@@ -11,10 +11,10 @@
  * known-answer tests for forces or integrators. The physics here is therefore
  * "parity unpinned" against the reference binary; it is pinned instead against
  * analytic known answers (two-particle forces/energies, lattice sums, Newton's
- * third law, FIRE two-particle minimum) in tests/test_oracle_*.py. The PFRAME
+ * third law, FIRE two-particle minimum) in tests/test_oracle.py. The PFRAME
  * and config-JSON formats ARE pinned against the reference's own
- * src/md_common.cpp and src/md_config.cpp, compiled from /root/reference by
- * oracle/build_ref.sh into oracle/_ref/.
+ * src/md_common.cpp and src/md_config.cpp, compiled from the reference tree by
+ * oracle/build_ref.py into oracle/_ref/ (tests/test_formats.py).
  *
  * Arithmetic modes:
  *  OR_FP64      every operation in double (the truth the force-error bound is
