@@ -304,6 +304,30 @@ int mdb_cell_build(const double* pos, int64_t n, double Lx, double Ly, double ce
                    int32_t device, int32_t* cell_out, int32_t* perm_out, int32_t* ncx_out,
                    int32_t* ncy_out);
 
+/* ---- forces without allocation ------------------------------------------
+ * No counterpart in the reference: an added entry point for callers that
+ * cannot allocate device memory — hosts whose own pool or caching allocator
+ * owns the device memory and forbids allocations behind its back, and loops
+ * that must not stall other streams on the implicit synchronisation of
+ * cudaMalloc/cudaFree. It computes what mdb_compute_forces computes, from
+ * device buffers the caller owns, on the caller's stream (`stream` is a
+ * cudaStream_t; NULL = the legacy default stream), and returns without
+ * synchronising. It calls no cudaMalloc, cudaFree or other allocating routine.
+ *   pos  device, 2n doubles (x0,y0,x1,y1,...)   type device, n int32
+ *   acc  device, 2n doubles out: F/m            uw   device, 2 doubles out:
+ *        U (shifted pair energy), W = sum_i 1/2 sum_j r.F
+ * Limit: n <= MDB_NOALLOC_MAX_PARTICLES (larger n returns MDB_ERR_CAPACITY
+ * before any work), because its scratch memory is one fixed 1 MiB device
+ * array inside the library. Every call on a device shares that array: calls
+ * ordered on one stream are independent (each clears what must start at
+ * zero), calls that overlap on the GPU race and give wrong results. The
+ * first call on a device (with that device current) looks the array's
+ * address up; make that first call before any stream capture. */
+#define MDB_NOALLOC_MAX_PARTICLES 65536
+int mdb_compute_forces_noalloc(const mdb_config_t* cfg, const double* pos, const int32_t* type,
+                               int64_t n, double Lx, double Ly, int32_t periodic_y, void* stream,
+                               double* acc, double* uw);
+
 /* ---- misc --------------------------------------------------------------- */
 /* Copies the last error message of the calling thread (NUL-terminated). */
 int mdb_last_error(char* buf, size_t cap);

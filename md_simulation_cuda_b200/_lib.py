@@ -202,6 +202,8 @@ SIGNATURES = {
                             _dp, _dp], C.c_int),
     "mdb_cell_build": ([_dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int32, _ip, _ip,
                         _ip, _ip], C.c_int),
+    "mdb_compute_forces_noalloc": ([_cfgp, _vp, _vp, C.c_int64, C.c_double, C.c_double, C.c_int32,
+                                    _vp, _vp, _vp], C.c_int),
     "mdb_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
     "mdb_version": ([], C.c_char_p),
     "mdb_kernel_launches": ([], C.c_int64),
