@@ -40,10 +40,11 @@ int reference_initial_frame(const mdb_config_t& cfg, std::vector<mdb_particle_t>
   const int N0 = cfg.n_particles_type0;
   const int N1 = N - N0;
   const double Lx = cfg.box_w_global, Ly = cfg.box_h_global;
-  if (N <= 0 || N0 <= 0 || N1 <= 0 || !(Lx > 0.0) || !(Ly > 0.0))
+  if (!(Lx > 0.0) || !(Ly > 0.0) || !std::isfinite(Lx) || !std::isfinite(Ly))
+    return set_error(MDB_ERR_BOX, "box_w_global and box_h_global must be positive");
+  if (N <= 0 || N0 <= 0 || N1 <= 0)
     return set_error(MDB_ERR_CONFIG,
-                     "lattice initialisation needs n_particles_global > n_particles_type0 > 0 "
-                     "and a positive box");
+                     "lattice initialisation needs n_particles_global > n_particles_type0 > 0");
   out.assign((size_t)N, mdb_particle_t{});
   const double band = Lx * cfg.devide_p;
   const double shift = Lx * (0.5 - cfg.devide_p / 2.0);

@@ -27,6 +27,8 @@ constexpr int kScanItems = 4;  // cells per thread in the scan kernels
 constexpr int kScanBlock = 512;
 constexpr int kScanTile = kScanItems * kScanBlock;
 constexpr int kGroup = 64;     // blocks per first-level reduction group
+// ncount[] flag: the list needs neither the minimum image nor offset wrapping.
+constexpr int32_t kListInterior = 1 << 30;
 
 // Force-phase variants.
 enum FMode : int32_t {
@@ -122,7 +124,7 @@ struct Dev {
   int32_t* perm;
   int32_t* nlist;     // neighbour list, offset j - i of entry k of slot i at
   int16_t* nlist16;   //   nlist[k * ntot + i] (int32) or nlist16[...] (int16)
-  int32_t* ncount;    // list length per slot, -1: use the cell stencil
+  int32_t* ncount;    // list length per slot (| kListInterior), -1: use the cell stencil
   int32_t max_nbr;
   int32_t nl16;       // 1: 16-bit offsets (every stencil offset fits in int16)
   int32_t* ccount;

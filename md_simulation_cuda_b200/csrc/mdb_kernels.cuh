@@ -315,8 +315,9 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
 // partner j from i inside the system's slot range, taken modulo the system
 // size n into [-n/2, n/2) (so the stencil rows across the periodic y edge stay
 // small): int16 at nlist16[k * ntot + i] when the batch uses 16-bit offsets,
-// else int32 at nlist[k * ntot + i]. Offsets are fetched eight at a time
-// before the dependent position gathers to keep several loads in flight.
+// else int32 at nlist[k * ntot + i]. MIC = false is the interior form: no
+// minimum image and no offset wrap (j = i + d). Offsets are fetched several at
+// a time before the dependent position gathers to keep loads in flight.
 template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
@@ -324,16 +325,20 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           float& fxc, float& fys, float& fyc, float& ws,
                                           float& wc, double& u) {
   const IDX* __restrict__ p = nlist + i;
-  const float4* __restrict__ base = pff + (i - li);  // slot 0 of the system
+  // MIC: slot 0 of the system and a wrapped index; interior: slot i itself
+  const float4* __restrict__ base = MIC ? pff + (i - li) : pff + i;
   constexpr int PF = (ENERGY || VIRIAL) ? 4 : 8;  // prefetch width (register budget)
   int k = 0;
   for (; k + PF <= nn; k += PF) {
     int j[PF];
 #pragma unroll
     for (int q = 0; q < PF; ++q) {
-      int t = li + (int)__ldg(p + (int64_t)(k + q) * ntot);
-      t += (t < 0) ? n : 0;
-      t -= (t >= n) ? n : 0;
+      int t = (int)__ldg(p + (int64_t)(k + q) * ntot);
+      if (MIC) {
+        t += li;
+        t += (t < 0) ? n : 0;
+        t -= (t >= n) ? n : 0;
+      }
       j[q] = t;
     }
 #pragma unroll
@@ -341,9 +346,12 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
       pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u);
   }
   for (; k < nn; ++k) {
-    int t = li + (int)__ldg(p + (int64_t)k * ntot);
-    t += (t < 0) ? n : 0;
-    t -= (t >= n) ? n : 0;
+    int t = (int)__ldg(p + (int64_t)k * ntot);
+    if (MIC) {
+      t += li;
+      t += (t < 0) ? n : 0;
+      t -= (t >= n) ? n : 0;
+    }
     pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u);
   }
 }
@@ -393,24 +401,19 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   float fxs = 0.f, fxc = 0.f, fys = 0.f, fyc = 0.f, ws = 0.f, wc = 0.f;
   u = 0.0;
   const float4* __restrict__ pff = D.pff;
-  const int nn = __ldg(D.ncount + i);
-  if (nn >= 0) {
+  const int nc = __ldg(D.ncount + i);
+  if (nc >= 0) {
     const int li = (int)(i - P.p0);
-    // Interior build cells (two or more cells from each periodic edge): the
-    // list partners were binned one cell away at most and move less than
-    // half a cell before the next rebuild, so no pair straddles an edge.
-    const int cell = __ldg(D.cell_of + i);
-    const int cx = cell % S.ncx, cy = cell / S.ncx;
-    const bool interior = cx >= 2 && cx <= S.ncx - 3 && (!PY || (cy >= 2 && cy <= S.ncy - 3));
+    const int nn = nc & (kListInterior - 1);
     if (D.nl16) {
-      if (interior)
+      if (nc & kListInterior)
         pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                              fys, fyc, ws, wc, u);
       else
         pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                             fys, fyc, ws, wc, u);
     } else {
-      if (interior)
+      if (nc & kListInterior)
         pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                              fys, fyc, ws, wc, u);
       else
@@ -1149,7 +1152,7 @@ __global__ void k_rb_copyback(Dev D) {
 // (rc_ij + skin), same displacement arithmetic as the force loop.
 template <bool PY>
 __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, const SysState& S,
-                                          int64_t k) {
+                                          int64_t k, int& nowrap) {
   PairCtx c;
   const float4 qi = D.pff[k];
   c.xih = fabsf(qi.x);
@@ -1168,6 +1171,7 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
   int cnt = 0;
   const int maxn = D.max_nbr;
   const int half = (P.n + 1) / 2;
+  nowrap = 1;
   for (int dr = -1; dr <= 1; ++dr) {
     int yy = cy + dr;
     if (PY) {
@@ -1205,8 +1209,14 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
         const float rl2 = (tj == ts) ? rl2s : rl2ab;
         if (r2 < rl2) {
           int d = j - (int)k;  // offset modulo n into [-n/2, n/2)
-          if (d >= half) d -= P.n;
-          if (d < -half) d += P.n;
+          if (d >= half) {
+            d -= P.n;
+            nowrap = 0;
+          }
+          if (d < -half) {
+            d += P.n;
+            nowrap = 0;
+          }
           if (D.nl16 && (d > 32767 || d < -32768)) return maxn + 1;  // use the stencil
           if (cnt < maxn) {
             if (D.nl16)
@@ -1234,13 +1244,23 @@ __global__ void k_rb_nlist(Dev D) {
       D.ncount[k] = -1;
       continue;
     }
-    const int cnt = S->periodic_y ? build_list<true>(D, P, *S, k) : build_list<false>(D, P, *S, k);
+    int nowrap = 0;
+    const int cnt = S->periodic_y ? build_list<true>(D, P, *S, k, nowrap)
+                                  : build_list<false>(D, P, *S, k, nowrap);
     if (cnt > D.max_nbr) {
       D.ncount[k] = -1;  // too many neighbours: the force loop scans the stencil
       atomicAdd(&S->nl_overflow, 1);
-    } else {
-      D.ncount[k] = cnt;
+      continue;
     }
+    // Interior build cells (two or more cells from each periodic edge) with
+    // unwrapped offsets: the partners were binned one cell away at most and
+    // move less than half a cell before the next rebuild, so no pair needs
+    // the minimum image and j = k + offset directly.
+    const int cell = D.cell_of[k];
+    const int cx = cell % S->ncx, cy = cell / S->ncx;
+    const bool interior = cx >= 2 && cx <= S->ncx - 3 &&
+                          (!S->periodic_y || (cy >= 2 && cy <= S->ncy - 3));
+    D.ncount[k] = cnt | ((interior && nowrap) ? kListInterior : 0);
   }
 }
 
