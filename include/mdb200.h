@@ -271,7 +271,12 @@ int mdb_batch_destroy(mdb_batch_t* b);
 int mdb_batch_add_fire(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
                        int64_t n, double force_tol, int32_t max_steps,
                        const mdb_fire_params_t* params, int32_t* sys_id);
-/* Add an MD segment of nsteps steps (MDB_JOB_NVE or MDB_JOB_NVT). */
+/* Add an MD segment: nsteps repetitions of step_single_NVE (MDB_JOB_NVE) or
+ * step_single_nose_hoover (MDB_JOB_NVT) (src/md_env.cu:1576-1728) from the
+ * given frame, with the constructor's initial force evaluation
+ * (src/md_env.cu:61-79). g = 2n - 2 uses this system's n. Every system of a
+ * batch has the same kind (FIRE, NVE or NVT); mixing returns MDB_ERR_STATE.
+ * A system stops after its own nsteps while the others continue. */
 int mdb_batch_add_md(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
                      int64_t n, int32_t kind, int64_t nsteps, int32_t* sys_id);
 /* Advance every unfinished system by up to `iterations` iterations (FIRE
@@ -284,7 +289,105 @@ int mdb_batch_system_info(mdb_batch_t* b, int32_t sys_id, int64_t* n, int32_t* d
 int mdb_batch_get_frame(mdb_batch_t* b, int32_t sys_id, mdb_particle_t* out, int64_t n);
 int mdb_batch_get_fire_result(mdb_batch_t* b, int32_t sys_id, mdb_minimize_result_t* result,
                               int32_t* energy_steps, double* energy_trace, int64_t trace_cap);
+/* cal_total_K / cal_total_U (src/md_env.cu:2141-2146, 2347-2360) and the
+ * Nose-Hoover xi of one system, or of every system (arrays of n = number of
+ * systems; any pointer may be NULL). */
+int mdb_batch_energies(mdb_batch_t* b, int32_t sys_id, double* K, double* U, double* xi);
+int mdb_batch_energies_all(mdb_batch_t* b, double* K, double* U, double* xi, int32_t n);
+/* Asynchronous form of mdb_batch_run (no counterpart in the reference): issue
+ * one chunk of at most `iterations` (< 0: no limit) iterations, ending at the
+ * next multiple of 1000, on the batch's stream and return at once; `issued`
+ * receives its length (0 when every system has finished). mdb_batch_query
+ * reports whether the stream has finished (idle = 1) without waiting;
+ * mdb_batch_collect then records finished systems and FIRE energy samples. */
+int mdb_batch_issue(mdb_batch_t* b, int64_t iterations, int64_t* issued);
+int mdb_batch_query(mdb_batch_t* b, int32_t* idle);
+int mdb_batch_collect(mdb_batch_t* b);
+/* Which systems have finished, as of the last run or collect (n = number of
+ * systems). */
+int mdb_batch_done_flags(mdb_batch_t* b, int32_t* done, int32_t n);
+/* Device memory the batch holds (0 before its first run). */
+int mdb_batch_device_bytes(mdb_batch_t* b, int64_t* bytes);
 int mdb_batch_cuda_stream(mdb_batch_t* b, void** stream);
+
+/* ---- serving: continuous batching of MD and FIRE requests ------------------
+ * No counterpart in the reference (which runs one MPI job per simulation). A
+ * server owns one worker thread and one device. Requests (an MD segment or a
+ * FIRE quench, each with its own config and frame) wait in a FIFO queue; while
+ * fewer than max_active_batches batches are in flight and the HBM budget
+ * allows, the oldest request and the following queued requests of the same
+ * kind are admitted together as a new batch on its own stream, so requests
+ * admitted at different times run concurrently. Results (frame and
+ * observables) become available as soon as the request's own system
+ * finishes; a batch's device memory is released when all of its systems
+ * have. A request's result equals that of the same job run alone
+ * (mdb_batch_* with one system, or mdb_sim_* / mdb_fire_minimize). All
+ * functions are thread-safe. */
+typedef struct mdb_server mdb_server_t;
+
+typedef struct mdb_server_options {
+  int32_t device;              /* CUDA device ordinal (default 0)               */
+  int32_t max_active_batches;  /* batches in flight at once (default 8)         */
+  int64_t hbm_budget_bytes;    /* device memory for batches (0: 80% of free)    */
+  int64_t max_batch_particles; /* particles per admitted batch (default 8Mi)    */
+  int32_t max_batch_systems;   /* systems per admitted batch (default 1024)     */
+  int32_t chunk;               /* steps / iterations issued per chunk (500)     */
+  double skin;                 /* as mdb_options_t                               */
+  int32_t use_graphs;
+  int32_t max_neighbors;
+  int32_t reserved[8];
+} mdb_server_options_t;
+
+typedef struct mdb_request {
+  int32_t kind;            /* MDB_JOB_FIRE, MDB_JOB_NVE or MDB_JOB_NVT          */
+  int32_t max_steps;       /* FIRE: iteration cap                                */
+  int64_t nsteps;          /* NVE/NVT: segment length in steps                   */
+  double force_tol;        /* FIRE: stop at max |a| < force_tol                  */
+  mdb_fire_params_t fire;  /* FIRE parameters                                    */
+} mdb_request_t;
+
+#define MDB_REQ_QUEUED 0
+#define MDB_REQ_RUNNING 1
+#define MDB_REQ_DONE 2
+#define MDB_REQ_FAILED 3
+
+typedef struct mdb_request_result {
+  int32_t status;     /* MDB_REQ_*                                              */
+  int32_t error;      /* status code of a failed request                         */
+  int64_t n;          /* particles                                               */
+  int64_t steps;      /* MD steps taken / FIRE iterations (as minimize_frame)    */
+  int32_t converged;  /* FIRE                                                    */
+  int32_t nonfinite;
+  double K, U, xi;    /* final kinetic and potential energy, Nose-Hoover xi      */
+  double max_force;   /* FIRE: max |a| at the end                                */
+  double t_submit, t_start, t_done; /* seconds since the server was created      */
+} mdb_request_result_t;
+
+typedef struct mdb_server_stats {
+  int64_t submitted, queued, running, finished, failed;
+  int64_t batches_admitted, active_batches;
+  int64_t device_bytes;      /* held by batches in flight                        */
+  int64_t hbm_budget_bytes;
+  double particle_steps;     /* sum of n x steps over finished requests          */
+  double elapsed_s;          /* since the server was created                     */
+} mdb_server_stats_t;
+
+void mdb_server_options_default(mdb_server_options_t* out);
+int mdb_server_create(const mdb_server_options_t* opt, mdb_server_t** out);
+/* Stops admitting, lets the chunks in flight end, fails what has not
+ * finished, joins the worker and frees everything. */
+int mdb_server_destroy(mdb_server_t* s);
+/* Queues a request (the frame is copied); its id goes to *id. */
+int mdb_server_submit(mdb_server_t* s, const mdb_config_t* cfg, const mdb_particle_t* frame,
+                      int64_t n, const mdb_request_t* req, int64_t* id);
+/* Waits until the request has finished or failed, or timeout_s seconds
+ * (< 0: no limit); *info receives its current record either way. */
+int mdb_server_wait(mdb_server_t* s, int64_t id, double timeout_s, mdb_request_result_t* info);
+/* The result of a finished request: frame_out (n particles, may be NULL) and
+ * *info; releases the request. A failed request returns its error status. */
+int mdb_server_result(mdb_server_t* s, int64_t id, mdb_particle_t* frame_out, int64_t n,
+                      mdb_request_result_t* info);
+int mdb_server_stats(mdb_server_t* s, mdb_server_stats_t* out);
 
 /* ---- single-call kernels (building blocks, used by tests) ------------------
  */

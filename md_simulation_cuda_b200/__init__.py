@@ -25,7 +25,12 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from ._lib import (MDB_ERR_ARG, MDBConfigC, MDBError, MDBFireParams, MDBMinimizeResult,
-                   MDBObservables, PARTICLE_DTYPE, check, frame_ptr, lib, options)
+                   MDBObservables, MDBRequest, MDBRequestResult, MDBServerOptions,
+                   MDBServerStats, PARTICLE_DTYPE, check, frame_ptr, lib, options)
+
+# job kinds (mdb200.h MDB_JOB_*) and request states (MDB_REQ_*)
+JOB_FIRE, JOB_NVE, JOB_NVT = 0, 1, 2
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 __all__ = [
     "PARTICLE_DTYPE", "MDBError", "MDConfig", "MDConfigManager", "MDSimulation",
@@ -384,7 +389,8 @@ class FileReader:
 
 
 class Batch:
-    """Many independent FIRE quenches advanced together on one GPU."""
+    """Many independent systems advanced together on one GPU: FIRE quenches
+    (add_fire) or MD segments of one kind (add_md)."""
 
     def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True):
         self._h = C.c_void_p()
@@ -414,8 +420,54 @@ class Batch:
         self._caps.append(max_steps // 1000 + 4)
         return sid.value
 
+    def add_md(self, config, frame, kind: int, nsteps: int) -> int:
+        """An MD segment of nsteps NVE (JOB_NVE) or Nose-Hoover (JOB_NVT) steps."""
+        f = _as_frame(frame)
+        sid = C.c_int32()
+        check(lib().mdb_batch_add_md(self._h, C.byref(_config_of(config)), frame_ptr(f), len(f),
+                                     int(kind), int(nsteps), C.byref(sid)))
+        self._sizes.append(len(f))
+        self._caps.append(4)
+        return sid.value
+
     def run(self, iterations: int = -1) -> None:
         check(lib().mdb_batch_run(self._h, int(iterations)))
+
+    def issue(self, iterations: int = -1) -> int:
+        """Issue one chunk without waiting; returns its length."""
+        k = C.c_int64()
+        check(lib().mdb_batch_issue(self._h, int(iterations), C.byref(k)))
+        return k.value
+
+    def idle(self) -> bool:
+        v = C.c_int32()
+        check(lib().mdb_batch_query(self._h, C.byref(v)))
+        return bool(v.value)
+
+    def collect(self) -> None:
+        check(lib().mdb_batch_collect(self._h))
+
+    def done_flags(self) -> np.ndarray:
+        d = np.zeros(len(self._sizes), dtype=np.int32)
+        check(lib().mdb_batch_done_flags(self._h, d.ctypes.data_as(C.POINTER(C.c_int32)), len(d)))
+        return d.astype(bool)
+
+    def energies(self, sys_id: int):
+        """(K, U, xi) of one system."""
+        K, U, xi = C.c_double(), C.c_double(), C.c_double()
+        check(lib().mdb_batch_energies(self._h, sys_id, C.byref(K), C.byref(U), C.byref(xi)))
+        return K.value, U.value, xi.value
+
+    def system_info(self, sys_id: int):
+        """(n, done, steps) of one system."""
+        n, d, st = C.c_int64(), C.c_int32(), C.c_int64()
+        check(lib().mdb_batch_system_info(self._h, sys_id, C.byref(n), C.byref(d), C.byref(st)))
+        return n.value, bool(d.value), st.value
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        check(lib().mdb_batch_device_bytes(self._h, C.byref(b)))
+        return b.value
 
     def progress(self):
         a = C.c_int32()
@@ -447,6 +499,122 @@ class Batch:
         p = C.c_void_p()
         check(lib().mdb_batch_cuda_stream(self._h, C.byref(p)))
         return p.value or 0
+
+
+@dataclass
+class RequestResult:
+    """A finished request of a Server."""
+    status: int
+    n: int
+    steps: int
+    converged: bool
+    nonfinite: bool
+    K: float
+    U: float
+    xi: float
+    max_force: float
+    t_submit: float
+    t_start: float
+    t_done: float
+    frame: np.ndarray = field(repr=False, default=None)
+
+    @property
+    def latency(self) -> float:
+        """Seconds from submission to the result being available."""
+        return self.t_done - self.t_submit
+
+
+class Server:
+    """Continuous batching of MD segments and FIRE quenches on one GPU
+    (mdb_server_*): submit_*() queues a request and returns at once; requests
+    are admitted into batches by an HBM budget as slots and memory free up,
+    and run concurrently with the batches already on the device."""
+
+    def __init__(self, device: int = 0, max_active_batches: Optional[int] = None,
+                 hbm_budget_bytes: Optional[int] = None, max_batch_particles: Optional[int] = None,
+                 max_batch_systems: Optional[int] = None, chunk: Optional[int] = None,
+                 skin: Optional[float] = None, use_graphs: bool = True):
+        self._h = C.c_void_p()
+        o = MDBServerOptions()
+        lib().mdb_server_options_default(C.byref(o))
+        o.device = device
+        for name, v in (("max_active_batches", max_active_batches),
+                        ("hbm_budget_bytes", hbm_budget_bytes),
+                        ("max_batch_particles", max_batch_particles),
+                        ("max_batch_systems", max_batch_systems), ("chunk", chunk),
+                        ("skin", skin)):
+            if v is not None:
+                setattr(o, name, v)
+        o.use_graphs = 1 if use_graphs else 0
+        check(lib().mdb_server_create(C.byref(o), C.byref(self._h)))
+        self._n = {}
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().mdb_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _submit(self, config, frame, req: MDBRequest) -> int:
+        f = _as_frame(frame)
+        rid = C.c_int64()
+        check(lib().mdb_server_submit(self._h, C.byref(_config_of(config)), frame_ptr(f), len(f),
+                                      C.byref(req), C.byref(rid)))
+        self._n[rid.value] = len(f)
+        return rid.value
+
+    def submit_md(self, config, frame, nsteps: int, nose_hoover: bool = True) -> int:
+        req = MDBRequest()
+        req.kind = JOB_NVT if nose_hoover else JOB_NVE
+        req.nsteps = int(nsteps)
+        return self._submit(config, frame, req)
+
+    def submit_fire(self, config, frame, force_tol: float, max_steps: int,
+                    params: "FireParams") -> int:
+        req = MDBRequest()
+        req.kind = JOB_FIRE
+        req.max_steps = int(max_steps)
+        req.force_tol = float(force_tol)
+        req.fire = params._c()
+        return self._submit(config, frame, req)
+
+    def wait(self, rid: int, timeout: float = -1.0) -> int:
+        """Waits for a request (timeout < 0: no limit); returns its status."""
+        info = MDBRequestResult()
+        check(lib().mdb_server_wait(self._h, rid, float(timeout), C.byref(info)))
+        return info.status
+
+    def result(self, rid: int) -> RequestResult:
+        """The result of a finished request (raises for a failed one); releases it."""
+        n = self._n[rid]
+        f = make_frame(n)
+        info = MDBRequestResult()
+        try:
+            check(lib().mdb_server_result(self._h, rid, frame_ptr(f), n, C.byref(info)))
+        finally:
+            if info.status in (REQ_DONE, REQ_FAILED):
+                self._n.pop(rid, None)
+        return RequestResult(status=info.status, n=info.n, steps=info.steps,
+                             converged=bool(info.converged), nonfinite=bool(info.nonfinite),
+                             K=info.K, U=info.U, xi=info.xi, max_force=info.max_force,
+                             t_submit=info.t_submit, t_start=info.t_start, t_done=info.t_done,
+                             frame=f)
+
+    def stats(self) -> MDBServerStats:
+        st = MDBServerStats()
+        check(lib().mdb_server_stats(self._h, C.byref(st)))
+        return st
 
 
 def compute_forces(config, frame, Lx: float, Ly: float, periodic_y: bool = True,

@@ -146,6 +146,59 @@ class MDBMinimizeResult(C.Structure):
     ]
 
 
+class MDBServerOptions(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("max_active_batches", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+        ("max_batch_particles", C.c_int64),
+        ("max_batch_systems", C.c_int32),
+        ("chunk", C.c_int32),
+        ("skin", C.c_double),
+        ("use_graphs", C.c_int32),
+        ("max_neighbors", C.c_int32),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+class MDBRequest(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("max_steps", C.c_int32),
+        ("nsteps", C.c_int64),
+        ("force_tol", C.c_double),
+        ("fire", MDBFireParams),
+    ]
+
+
+class MDBRequestResult(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("error", C.c_int32),
+        ("n", C.c_int64),
+        ("steps", C.c_int64),
+        ("converged", C.c_int32),
+        ("nonfinite", C.c_int32),
+        ("K", C.c_double),
+        ("U", C.c_double),
+        ("xi", C.c_double),
+        ("max_force", C.c_double),
+        ("t_submit", C.c_double),
+        ("t_start", C.c_double),
+        ("t_done", C.c_double),
+    ]
+
+
+class MDBServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64), ("queued", C.c_int64), ("running", C.c_int64),
+        ("finished", C.c_int64), ("failed", C.c_int64),
+        ("batches_admitted", C.c_int64), ("active_batches", C.c_int64),
+        ("device_bytes", C.c_int64), ("hbm_budget_bytes", C.c_int64),
+        ("particle_steps", C.c_double), ("elapsed_s", C.c_double),
+    ]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -197,7 +250,23 @@ SIGNATURES = {
     "mdb_batch_system_info": ([_vp, C.c_int32, C.POINTER(C.c_int64), _ip, C.POINTER(C.c_int64)], C.c_int),
     "mdb_batch_get_frame": ([_vp, C.c_int32, _vp, C.c_int64], C.c_int),
     "mdb_batch_get_fire_result": ([_vp, C.c_int32, C.POINTER(MDBMinimizeResult), _ip, _dp, C.c_int64], C.c_int),
+    "mdb_batch_energies": ([_vp, C.c_int32, _dp, _dp, _dp], C.c_int),
+    "mdb_batch_energies_all": ([_vp, _dp, _dp, _dp, C.c_int32], C.c_int),
+    "mdb_batch_issue": ([_vp, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+    "mdb_batch_query": ([_vp, _ip], C.c_int),
+    "mdb_batch_collect": ([_vp], C.c_int),
+    "mdb_batch_done_flags": ([_vp, _ip, C.c_int32], C.c_int),
+    "mdb_batch_device_bytes": ([_vp, C.POINTER(C.c_int64)], C.c_int),
     "mdb_batch_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
+    "mdb_server_options_default": ([C.POINTER(MDBServerOptions)], None),
+    "mdb_server_create": ([C.POINTER(MDBServerOptions), C.POINTER(_vp)], C.c_int),
+    "mdb_server_destroy": ([_vp], C.c_int),
+    "mdb_server_submit": ([_vp, _cfgp, _vp, C.c_int64, C.POINTER(MDBRequest),
+                           C.POINTER(C.c_int64)], C.c_int),
+    "mdb_server_wait": ([_vp, C.c_int64, C.c_double, C.POINTER(MDBRequestResult)], C.c_int),
+    "mdb_server_result": ([_vp, C.c_int64, _vp, C.c_int64, C.POINTER(MDBRequestResult)],
+                          C.c_int),
+    "mdb_server_stats": ([_vp, C.POINTER(MDBServerStats)], C.c_int),
     "mdb_compute_forces": ([_cfgp, _vp, C.c_int64, C.c_double, C.c_double, C.c_int32, _optp, _dp,
                             _dp, _dp], C.c_int),
     "mdb_cell_build": ([_dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int32, _ip, _ip,

@@ -454,9 +454,10 @@ struct mdb_batch {
   std::unique_ptr<Engine> eng;
   std::vector<SystemSpec> pending;
   std::vector<Trace> traces;
-  std::vector<int32_t> recorded_done;  // final sample recorded
-  std::vector<int32_t> max_steps;
-  int64_t iter = 0;
+  std::vector<int32_t> recorded_done;  // FIRE: final sample recorded; MD: segment finished
+  std::vector<int32_t> max_steps;      // FIRE: iteration cap; MD: segment length
+  int32_t kind = -1;                   // K_FIRE, K_NVE or K_NVT, shared by every system
+  int64_t iter = 0;                    // iterations / steps issued so far
   bool built = false;
 };
 
@@ -472,9 +473,16 @@ int batch_build(mdb_batch_t* b) {
   MDB_TRY(b->eng->build());
   b->traces.assign(ns, Trace());
   b->recorded_done.assign(ns, 0);
-  std::vector<SysState> S;
-  MDB_TRY(obs_energies(*b->eng, S));
-  for (size_t s = 0; s < ns; ++s) b->traces[s].add(0, S[s].U);
+  if (b->kind == mdb::K_FIRE) {
+    std::vector<SysState> S;
+    MDB_TRY(obs_energies(*b->eng, S));
+    for (size_t s = 0; s < ns; ++s) b->traces[s].add(0, S[s].U);
+  } else {
+    // what the MDSimulation constructor leaves: forces, and K for the first
+    // Nose-Hoover half step
+    MDB_TRY(b->eng->force(mdb::FM_INIT, true));
+    if (b->kind == mdb::K_NVT) MDB_TRY(b->eng->reduce_K());
+  }
   b->built = true;
   return MDB_OK;
 }
@@ -483,13 +491,48 @@ bool fire_finished(const SysState& S, int32_t max_steps) {
   return S.f_conv != 0 || S.f_step >= max_steps || S.err != 0;
 }
 
-// Records convergence and periodic energy samples after a chunk that ended
-// at iteration b->iter.
+int32_t batch_cap(const mdb_batch_t* b) {
+  int32_t cap = 0;
+  for (int32_t m : b->max_steps) cap = m > cap ? m : cap;
+  return cap;
+}
+
+// Length of the next chunk: chunks end on multiples of 1000 iterations (the
+// energy samples of minimize_frame for FIRE; for MD, finished segments are
+// noticed at least that often).
+int64_t batch_next_chunk(const mdb_batch_t* b, int64_t left) {
+  const int64_t cap = batch_cap(b);
+  int64_t chunk = std::min<int64_t>(left, cap - b->iter);
+  chunk = std::min<int64_t>(chunk, 1000 - (b->iter % 1000));
+  return chunk;
+}
+
+// Issues one chunk on the batch's stream without waiting for it.
+int batch_issue(mdb_batch_t* b, int64_t chunk) {
+  if (chunk <= 0) return MDB_OK;
+  if (b->kind == mdb::K_FIRE) {
+    MDB_TRY(b->eng->run_fire(chunk));
+  } else if (b->kind == mdb::K_NVT) {
+    MDB_TRY(b->eng->run_md(mdb::DM_NH, mdb::FM_NH, true, chunk));
+  } else {
+    MDB_TRY(b->eng->run_md(mdb::DM_NVE, mdb::FM_NVE, true, chunk));
+  }
+  b->iter += chunk;
+  return MDB_OK;
+}
+
+// Records finished systems (and FIRE energy samples) after a chunk that ended
+// at iteration b->iter; waits for the batch's stream.
 int batch_harvest(mdb_batch_t* b) {
   std::vector<SysState> S;
   MDB_TRY(b->eng->get_states(S));
-  bool need_u = false;
   const size_t ns = S.size();
+  if (b->kind != mdb::K_FIRE) {
+    for (size_t s = 0; s < ns; ++s)
+      if (S[s].done || S[s].err) b->recorded_done[s] = 1;
+    return MDB_OK;
+  }
+  bool need_u = false;
   for (size_t s = 0; s < ns; ++s) {
     if (b->recorded_done[s]) continue;
     if (S[s].f_conv || S[s].f_step >= b->max_steps[s] || (b->iter % 1000 == 0)) need_u = true;
@@ -510,6 +553,23 @@ int batch_harvest(mdb_batch_t* b) {
       tr.add((int32_t)b->iter, U[s].U);
     }
   }
+  return MDB_OK;
+}
+
+bool batch_all_done(const mdb_batch_t* b) {
+  for (int32_t x : b->recorded_done)
+    if (!x) return false;
+  return true;
+}
+
+int batch_add(mdb_batch_t* b, SystemSpec&& spec, int32_t kind, int32_t cap, int32_t* sys_id) {
+  if (b->built) return mdb::set_error(MDB_ERR_STATE, "systems can only be added before the first run");
+  if (b->kind >= 0 && b->kind != kind)
+    return mdb::set_error(MDB_ERR_STATE, "every system of a batch must be of the same job kind");
+  b->kind = kind;
+  b->pending.push_back(std::move(spec));
+  b->max_steps.push_back(cap);
+  if (sys_id) *sys_id = (int32_t)b->pending.size() - 1;
   return MDB_OK;
 }
 
@@ -535,7 +595,6 @@ int mdb_batch_add_fire(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_partic
                        int64_t n, double force_tol, int32_t max_steps,
                        const mdb_fire_params_t* params, int32_t* sys_id) {
   if (!b || !cfg || !frame || !params || n <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
-  if (b->built) return mdb::set_error(MDB_ERR_STATE, "systems can only be added before the first run");
   if (max_steps <= 0) return mdb::set_error(MDB_ERR_ARG, "max_steps must be positive");
   SystemSpec spec;
   spec.cfg = *cfg;
@@ -545,41 +604,109 @@ int mdb_batch_add_fire(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_partic
   spec.tol = force_tol;
   spec.max_steps = max_steps;
   spec.fire_prepare = true;
-  b->pending.push_back(std::move(spec));
-  b->max_steps.push_back(max_steps);
-  if (sys_id) *sys_id = (int32_t)b->pending.size() - 1;
-  return MDB_OK;
+  return batch_add(b, std::move(spec), mdb::K_FIRE, max_steps, sys_id);
 }
 
 int mdb_batch_add_md(mdb_batch_t* b, const mdb_config_t* cfg, const mdb_particle_t* frame,
                      int64_t n, int32_t kind, int64_t nsteps, int32_t* sys_id) {
-  (void)b;
-  (void)cfg;
-  (void)frame;
-  (void)n;
-  (void)kind;
-  (void)nsteps;
-  (void)sys_id;
-  return mdb::set_error(MDB_ERR_STATE, "MD segments in batches are not available in this build");
+  if (!b || !cfg || !frame || n <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (kind != MDB_JOB_NVE && kind != MDB_JOB_NVT)
+    return mdb::set_error(MDB_ERR_ARG, "kind must be MDB_JOB_NVE or MDB_JOB_NVT");
+  if (nsteps <= 0 || nsteps > INT32_MAX) return mdb::set_error(MDB_ERR_ARG, "nsteps out of range");
+  SystemSpec spec;
+  spec.cfg = *cfg;
+  spec.cfg.n_particles_global = (int32_t)n;  // g = 2N - 2 counts this system
+  spec.frame.assign(frame, frame + n);
+  const int32_t k = kind == MDB_JOB_NVT ? mdb::K_NVT : mdb::K_NVE;
+  spec.kind = k;
+  spec.target_steps = nsteps;
+  return batch_add(b, std::move(spec), k, (int32_t)nsteps, sys_id);
 }
 
 int mdb_batch_run(mdb_batch_t* b, int64_t iterations) {
   if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
   MDB_TRY(batch_build(b));
-  int32_t cap = 0;
-  for (int32_t m : b->max_steps) cap = m > cap ? m : cap;
+  const int32_t cap = batch_cap(b);
   int64_t left = iterations < 0 ? (int64_t)cap - b->iter : iterations;
   while (left > 0 && b->iter < cap) {
-    const int64_t to_sample = 1000 - (b->iter % 1000);
-    const int64_t chunk = std::min<int64_t>(std::min<int64_t>(to_sample, left), (int64_t)cap - b->iter);
-    MDB_TRY(b->eng->run_fire(chunk));
-    b->iter += chunk;
+    const int64_t chunk = batch_next_chunk(b, left);
+    MDB_TRY(batch_issue(b, chunk));
     left -= chunk;
     MDB_TRY(batch_harvest(b));
-    bool all = true;
-    for (size_t s = 0; s < b->recorded_done.size(); ++s) all = all && b->recorded_done[s];
-    if (all) break;
+    if (batch_all_done(b)) break;
   }
+  return MDB_OK;
+}
+
+int mdb_batch_issue(mdb_batch_t* b, int64_t iterations, int64_t* issued) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  if (issued) *issued = 0;
+  MDB_TRY(batch_build(b));
+  const int64_t left = iterations < 0 ? (int64_t)batch_cap(b) - b->iter : iterations;
+  if (left <= 0 || batch_all_done(b)) return MDB_OK;
+  const int64_t chunk = batch_next_chunk(b, left);
+  MDB_TRY(batch_issue(b, chunk));
+  if (issued) *issued = chunk;
+  return MDB_OK;
+}
+
+int mdb_batch_query(mdb_batch_t* b, int32_t* idle) {
+  if (!b || !idle) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  if (!b->built) {
+    *idle = 1;
+    return MDB_OK;
+  }
+  bool v = false;
+  MDB_TRY(b->eng->idle(&v));
+  *idle = v ? 1 : 0;
+  return MDB_OK;
+}
+
+int mdb_batch_collect(mdb_batch_t* b) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  return batch_harvest(b);
+}
+
+int mdb_batch_energies_all(mdb_batch_t* b, double* K, double* U, double* xi, int32_t n) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (n != b->eng->nsys()) return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the number of systems");
+  std::vector<SysState> S;
+  MDB_TRY(obs_energies(*b->eng, S));
+  for (int32_t s = 0; s < n; ++s) {
+    if (K) K[s] = 0.5 * S[s].kin;
+    if (U) U[s] = S[s].U;
+    if (xi) xi[s] = S[s].xi;
+  }
+  return MDB_OK;
+}
+
+int mdb_batch_energies(mdb_batch_t* b, int32_t sys_id, double* K, double* U, double* xi) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (sys_id < 0 || sys_id >= b->eng->nsys()) return mdb::set_error(MDB_ERR_ARG, "bad system id");
+  std::vector<SysState> S;
+  MDB_TRY(obs_energies(*b->eng, S));
+  if (K) *K = 0.5 * S[sys_id].kin;
+  if (U) *U = S[sys_id].U;
+  if (xi) *xi = S[sys_id].xi;
+  if (S[sys_id].nonfinite) return mdb::set_error(MDB_ERR_NONFINITE, "non-finite state");
+  return MDB_OK;
+}
+
+int mdb_batch_done_flags(mdb_batch_t* b, int32_t* done, int32_t n) {
+  if (!b || !done) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (n != (int32_t)b->recorded_done.size())
+    return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the number of systems");
+  for (int32_t s = 0; s < n; ++s) done[s] = b->recorded_done[s] ? 1 : 0;
+  return MDB_OK;
+}
+
+int mdb_batch_device_bytes(mdb_batch_t* b, int64_t* bytes) {
+  if (!b || !bytes) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  *bytes = b->built ? b->eng->device_bytes() : 0;
   return MDB_OK;
 }
 
@@ -602,8 +729,13 @@ int mdb_batch_system_info(mdb_batch_t* b, int32_t sys_id, int64_t* n, int32_t* d
   SysState S;
   MDB_TRY(b->eng->get_state(sys_id, &S));
   if (n) *n = b->eng->n(sys_id);
-  if (done) *done = fire_finished(S, b->max_steps[sys_id]) ? 1 : 0;
-  if (steps) *steps = S.f_conv ? S.f_conv_step : S.f_step;
+  if (b->kind == mdb::K_FIRE) {
+    if (done) *done = fire_finished(S, b->max_steps[sys_id]) ? 1 : 0;
+    if (steps) *steps = S.f_conv ? S.f_conv_step : S.f_step;
+  } else {
+    if (done) *done = (S.done || S.err) ? 1 : 0;
+    if (steps) *steps = S.steps;
+  }
   return MDB_OK;
 }
 

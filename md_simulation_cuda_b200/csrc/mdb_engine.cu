@@ -223,6 +223,7 @@ int Engine::build() {
   auto alloc = [&](void** p, size_t bytes) -> int {
     MDB_CUDA(cudaMalloc(p, bytes < 16 ? 16 : bytes));
     allocs_.push_back(*p);
+    bytes_ += (int64_t)(bytes < 16 ? 16 : bytes);
     return MDB_OK;
   };
 #define MDB_ALLOC(ptr, count)                                                 \
@@ -658,6 +659,20 @@ int Engine::sync() {
   MDB_CUDA(cudaSetDevice(device_));
   MDB_CUDA(cudaStreamSynchronize(stream_));
   return MDB_OK;
+}
+
+int Engine::idle(bool* out) {
+  MDB_CUDA(cudaSetDevice(device_));
+  const cudaError_t e = cudaStreamQuery(stream_);
+  if (e == cudaSuccess) {
+    *out = true;
+    return MDB_OK;
+  }
+  if (e == cudaErrorNotReady) {
+    *out = false;
+    return MDB_OK;
+  }
+  return cuda_error(e, "cudaStreamQuery");
 }
 
 }  // namespace mdb

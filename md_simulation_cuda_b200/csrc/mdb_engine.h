@@ -66,6 +66,11 @@ class Engine {
   // Slot -> original index and slot -> local cell of system s (n entries each).
   int debug_cells(int s, int32_t* orig, int32_t* cell);
   int sync();
+  // Whether every issued kernel and copy of the engine's stream has finished
+  // (does not wait).
+  int idle(bool* out);
+  // Device memory the engine holds, in bytes.
+  int64_t device_bytes() const { return bytes_; }
 
   // Kernel launches issued (eager launches + kernel nodes of launched graphs,
   // counting the rebuild body once per rebuild actually run).
@@ -102,6 +107,7 @@ class Engine {
   std::vector<void*> allocs_;
   std::map<std::tuple<int, int, int, int, int>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
   long long launches_ = 0;
+  int64_t bytes_ = 0;
   long long last_rebuilds_ = 0;
 };
 

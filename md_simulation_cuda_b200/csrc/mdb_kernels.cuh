@@ -493,7 +493,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
-  const bool skip = (S->done != 0) || (S->err != 0) ||
+  // a finished batch system is still observed (FM_OBS) and re-evaluated (FM_INIT)
+  const bool skip = (FM != FM_OBS && FM != FM_INIT && S->done != 0) || (S->err != 0) ||
                     (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
   constexpr bool kEnergy = (FM == FM_OBS);
   constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
@@ -638,7 +639,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
         S->f_step += 1;
       }
     }
-    if (FM != FM_INIT && FM != FM_OBS && FM != FM_FIRE) S->steps += 1;
+    if (FM != FM_INIT && FM != FM_OBS && FM != FM_FIRE) {
+      S->steps += 1;
+      // an MD segment of a batch ends after its target number of steps
+      if (P.target_steps > 0 && S->steps >= P.target_steps) S->done = 1;
+    }
   }
   if (FM == FM_FIRE) S->f_drift = (!skip && !S->f_conv) ? 1 : 0;
   S->counter = 0u;

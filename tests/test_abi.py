@@ -49,3 +49,39 @@ def test_errors_are_status_codes_without_gpu(built):
     assert L.mdb_sim_step_nve(None, 1) == _lib.MDB_ERR_ARG
     assert "bad arguments" in _lib.last_error()
     assert L.mdb_version().startswith(b"mdb200")
+
+
+def test_batch_kinds_cannot_mix_without_gpu(built):
+    """Adding systems only stores them (no device work): a batch holds one job
+    kind, and MD segments need a positive length."""
+    import md_simulation_cuda_b200 as m
+    from md_simulation_cuda_b200 import workloads as wl
+
+    f, L = wl.random_frame(50, 0.7, 0.5, 3)
+    cfg = wl.config_dict(50, L, L, dt=0.001, T=0.0)
+    b = m.Batch()
+    b.add_md(cfg, f, m.JOB_NVT, 10)
+    try:
+        b.add_fire(cfg, f, 1e-4, 100, m.FireParams.from_config(cfg))
+        raise AssertionError("mixed kinds accepted")
+    except m.MDBError as e:
+        assert e.code == _lib.MDB_ERR_STATE
+    try:
+        b.add_md(cfg, f, m.JOB_NVT, 0)
+        raise AssertionError("zero-length segment accepted")
+    except m.MDBError as e:
+        assert e.code == _lib.MDB_ERR_ARG
+
+
+def test_server_needs_a_device(built):
+    import torch
+
+    import md_simulation_cuda_b200 as m
+
+    if torch.cuda.is_available():
+        return  # the GPU server tests cover this case
+    try:
+        m.Server()
+        raise AssertionError("server created without a device")
+    except m.MDBError as e:
+        assert e.code == _lib.MDB_ERR_NODEVICE
