@@ -136,6 +136,183 @@ def cpu_cell_baseline(f, cfg, mode_name, budget_s=20.0):
                       f"(reference mixed-precision pair arithmetic, OpenMP on all cores)"}
 
 
+def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=False):
+    """C4: the 512-system FIRE mix as ONE batch vs the same systems run one at
+    a time through the single-system path (a stratified sample of
+    `plain_sample` systems, each as a batch of one). particle-iterations are
+    counted per system from its own iteration counter, so systems that
+    converge stop counting. Wall clock around synchronous runs."""
+    import numpy as np
+
+    import md_simulation_cuda_b200 as mdb
+    from md_simulation_cuda_b200 import workloads as wl
+
+    S = wl.FIRE_SETTINGS
+    params = wl.fire_params()
+    systems = wl.fire_mix(512)
+    sizes = np.array([len(f) for f, _ in systems])
+
+    def steps_of(b, ids):
+        return np.array([b.system_info(i)[2] for i in ids], dtype=np.int64)
+
+    b = mdb.Batch(device=dev)
+    ids = [b.add_fire(cfg, f, S["force_tol"], S["max_steps"], params) for f, cfg in systems]
+    t_build = time.perf_counter()
+    b.run(warm_iters)
+    t_build = time.perf_counter() - t_build
+    s0 = steps_of(b, ids)
+    t0 = time.perf_counter()
+    b.run(-1 if to_completion else iters)
+    t_batch = time.perf_counter() - t0
+    s1 = steps_of(b, ids)
+    work = float((sizes * (s1 - s0)).sum())
+    done = int(b.progress()[1])
+    converged = sum(1 for i in ids if b.system_info(i)[1] and b.system_info(i)[2] < S["max_steps"])
+    del b
+    # plain path: the same window for a stratified sample, one system at a time
+    order = np.argsort(sizes)
+    pick = order[:: max(1, len(order) // plain_sample)][:plain_sample]
+    p_work, p_time = 0.0, 0.0
+    for k in pick:
+        f, cfg = systems[k]
+        one = mdb.Batch(device=dev)
+        one.add_fire(cfg, f, S["force_tol"], S["max_steps"], params)
+        one.run(warm_iters)
+        a0 = one.system_info(0)[2]
+        t1 = time.perf_counter()
+        one.run(-1 if to_completion else iters)
+        p_time += time.perf_counter() - t1
+        p_work += float(sizes[k] * (one.system_info(0)[2] - a0))
+        del one
+    plain = p_work / p_time if p_time > 0 else None
+    value = work / t_batch
+    return {"metric": "particle-iterations/s", "value": value, "unit": "particle-iterations/s",
+            "systems": len(systems), "particles": int(sizes.sum()),
+            "window": ("to completion" if to_completion else f"iterations {warm_iters}.."
+                       f"{warm_iters + iters}"),
+            "seconds": t_batch, "build_and_warmup_s": t_build,
+            "finished_systems": done, "converged_systems": converged,
+            "plain_path": {"value": plain, "unit": "particle-iterations/s",
+                           "sample": f"{len(pick)} systems (every {max(1, len(order) // plain_sample)}"
+                                     f"th by N), each alone as a batch of one, same window"},
+            "ratio_vs_plain": (value / plain) if plain else None}
+
+
+def run_fire_mix(args):
+    import torch
+
+    ws, rank, local = _dist()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    res = measure_fire_mix(0, args.warmup, args.steps, to_completion=args.to_completion)
+    clk = clocks.stop()
+    out = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "fp32-pair/fp64-state",
+           "data": "synthetic (seeded uniform-random starts)",
+           "config": {"workload": "batched FIRE, 512 systems, N log-uniform [256, 16384], "
+                                  "f_A ~ U(0.2,0.8), rho ~ U(0.6,1.0), square periodic boxes, "
+                                  "uniform-random positions; dt_init 0.001, dt_max 0.01, "
+                                  "alpha0 0.1, f_inc 1.1, f_dec 0.5, tol 1e-6, 20000 its"},
+           "batched": res, "clocks": clk}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_served(args):
+    """C5: the served mixed stream through mdb.Server (continuous batching).
+    Requests are submitted at their Poisson arrival times by one thread while
+    a pool of threads builds their frames ahead of time; latency is measured
+    from the scheduled arrival to the result being available on the host."""
+    import queue
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+    import torch
+
+    import md_simulation_cuda_b200 as mdb
+    from md_simulation_cuda_b200 import workloads as wl
+
+    ws, rank, local = _dist()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    specs = wl.served_stream(n_requests=args.requests)
+    params = wl.fire_params()
+    S = wl.FIRE_SETTINGS
+    pool = ThreadPoolExecutor(max_workers=8)
+    futures = [pool.submit(wl.served_frame, sp) for sp in specs[:64]]
+    nxt = len(futures)
+    srv = mdb.Server(device=0)
+    host_t0 = time.perf_counter()  # the server clock starts at creation
+    ids = queue.Queue()
+    clocks = ClockSampler(0)
+    clocks.start()
+    start = time.perf_counter()
+    lag = []
+    for k, sp in enumerate(specs):
+        f, cfg = futures[k].result()
+        futures[k] = None
+        if nxt < len(specs):
+            futures.append(pool.submit(wl.served_frame, specs[nxt]))
+            nxt += 1
+        delay = start + sp["arrival"] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        lag.append(max(0.0, -delay))
+        if sp["fire"]:
+            rid = srv.submit_fire(cfg, f, S["force_tol"], S["max_steps"], params)
+        else:
+            rid = srv.submit_md(cfg, f, sp["steps"], nose_hoover=True)
+        ids.put((k, rid))
+    ids.put(None)
+    results = {}
+    while True:
+        item = ids.get()
+        if item is None:
+            break
+        k, rid = item
+        srv.wait(rid)
+        r = srv.result(rid)
+        r.frame = None
+        results[k] = r
+    clk = clocks.stop()
+    st = srv.stats()
+    srv.close()
+    pool.shutdown()
+    offset = start - host_t0
+    lat = np.array([results[k].t_done - (offset + specs[k]["arrival"]) for k in results])
+    lat_fire = np.array([lat[i] for i, k in enumerate(results) if specs[k]["fire"]])
+    lat_md = np.array([lat[i] for i, k in enumerate(results) if not specs[k]["fire"]])
+    work = sum(results[k].n * results[k].steps for k in results)
+    t_first = offset + specs[0]["arrival"]
+    t_last = max(results[k].t_done for k in results)
+    agg = work / (t_last - t_first)
+    out = {"metric": "served particle-steps/s (p50/p99 latency)", "value": agg,
+           "unit": "particle-steps/s", "n_gpus": 1, "steps": len(specs), "warmup": 0,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32-pair/fp64-state", "data": "synthetic (seeded jittered lattices)",
+           "config": {"workload": f"served stream: {len(specs)} requests, Poisson 200/s, 70% NVT "
+                                  "(N log-uniform [1024, 262144], 1000-20000 steps, T ~ U(0.5,1.2)) "
+                                  "/ 30% FIRE quench (same N law, tol 1e-6, 20000 its)",
+                      "server": "mdb.Server defaults (8 batches in flight, 80% of free HBM)"},
+           "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                         "max": float(lat.max()),
+                         "nvt_p50": float(np.percentile(lat_md, 50)) if len(lat_md) else None,
+                         "fire_p50": float(np.percentile(lat_fire, 50)) if len(lat_fire) else None,
+                         "from": "scheduled arrival to result on the host"},
+           "arrival_lag_s": {"p50": float(np.percentile(lag, 50)), "max": float(max(lag))},
+           "requests": {"finished": int(st.finished), "failed": int(st.failed),
+                        "batches_admitted": int(st.batches_admitted)},
+           "wall_s": t_last - t_first, "clocks": clk}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_reference(args):
     """Reference arm: the O(N^2) all-pairs force loop, bounded row sample."""
     ws, rank, _ = _dist()
@@ -289,6 +466,11 @@ def run_ours(args):
            "how": "set_frame from pinned host memory, K steps each followed by an "
                   "observables read, get_frame; wall clock"}
 
+    # ---- C4: the 512-system FIRE mix, batched vs one system at a time --------
+    batched = None
+    if rank == 0 and ws == 1 and args.workload == "nvt_slab":
+        batched = measure_fire_mix(dev, 100, 2000)
+
     if rank == 0:
         achieved = force_bytes / t_force / 1e9
         out = {
@@ -314,6 +496,7 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clk,
+            "batched": batched,
         }
         print(json.dumps(out), flush=True)
     del sim
@@ -328,11 +511,19 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="nvt_slab", choices=["nvt_slab", "nve_4096"])
+    ap.add_argument("--workload", default="nvt_slab",
+                    choices=["nvt_slab", "nve_4096", "fire_mix", "served"])
+    ap.add_argument("--to-completion", action="store_true",
+                    help="fire_mix: run every system until it converges or hits 20000 its")
+    ap.add_argument("--requests", type=int, default=2000, help="served: number of requests")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "fire_mix":
+        return run_fire_mix(args)
+    if args.workload == "served":
+        return run_served(args)
     return run_ours(args)
 
 

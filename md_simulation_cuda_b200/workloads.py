@@ -117,3 +117,42 @@ def fire_mix(n_systems: int = 512, seed: int = 4, n_min: int = 256, n_max: int =
 
 FIRE_SETTINGS = dict(dt_init=0.001, dt_max=0.01, alpha0=0.1, f_inc=1.1, f_dec=0.5, N_min=5,
                      force_tol=1e-6, max_steps=20000)
+
+
+def fire_params():
+    """FireParams of the batched FIRE mix and the served FIRE quenches."""
+    from . import FireParams
+
+    s = FIRE_SETTINGS
+    return FireParams(dt_init=s["dt_init"], dt_max=s["dt_max"], alpha0=s["alpha0"],
+                      f_inc=s["f_inc"], f_dec=s["f_dec"], N_min=s["N_min"])
+
+
+def served_stream(n_requests: int = 2000, rate: float = 200.0, seed: int = 5,
+                  fire_fraction: float = 0.3, n_min: int = 1024, n_max: int = 262144):
+    """Request specs of the served mixed stream: Poisson arrivals at `rate`
+    per second; NVT segments (N log-uniform in [n_min, n_max], 1000-20000
+    steps, T ~ U(0.5, 1.2)) or FIRE quenches (fire_fraction of requests, same
+    N law), each from a jittered-lattice start with its own seed. Frames are
+    made on demand by served_frame(spec)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        N = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        fire = bool(rng.random() < fire_fraction)
+        steps = int(rng.integers(1000, 20001))
+        T = float(rng.uniform(0.5, 1.2))
+        out.append(dict(k=k, arrival=t, N=N, fire=fire, steps=steps, T=T,
+                        seed=seed * 1000003 + k))
+    return out
+
+
+def served_frame(spec):
+    """(frame, config dict) of one served request: rho = 0.8, 65% A, square
+    box, lattice jitter +-0.1; FIRE quenches start at rest."""
+    T = 0.0 if spec["fire"] else spec["T"]
+    f, Lx, Ly = lattice_frame(spec["N"], 0.8, 1.0, 0.65, T, spec["seed"], jitter=0.1)
+    return f, config_dict(spec["N"], Lx, Ly, dt=0.002 if not spec["fire"] else 0.001,
+                          T=spec["T"], Q=1.0, n_cap=spec["N"])
