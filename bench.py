@@ -51,6 +51,31 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The maximum of x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def lpt_assign(costs, nbins):
+    """Greedy longest-processing-time assignment of independent systems to
+    ranks: largest cost first, each to the least-loaded rank (ties to the
+    lower rank). Returns the rank of every system."""
+    order = sorted(range(len(costs)), key=lambda k: (-costs[k], k))
+    load = [0.0] * nbins
+    out = [0] * len(costs)
+    for k in order:
+        r = min(range(nbins), key=lambda b: (load[b], b))
+        out[k] = r
+        load[r] += costs[k]
+    return out
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -111,6 +136,10 @@ def make_workload(name, rank):
     if name == "nve_4096":
         f, cfg = wl.nve_4096(seed=1 + 1000 * rank)
         return f, cfg, "nve", "NVE velocity Verlet N=4096, rho=0.8, dt=0.001"
+    if name == "nph_4m":
+        f, cfg = wl.nph_square(seed=3 + 1000 * rank)
+        return f, cfg, "nph", ("NPH barostat N=4194304, square box, rho=0.8, 65% A, P_ext=1.0, "
+                               "W=10.0, dt=0.001")
     f, cfg = wl.nvt_slab(seed=2 + 1000 * rank)
     return f, cfg, "nh", ("Nose-Hoover interface slab N=1048576, Lx=2Ly, rho=0.8, "
                           "90%/10% A stripes, T=0.7, Q=1.0, dt=0.002")
@@ -121,7 +150,12 @@ def cpu_cell_baseline(f, cfg, mode_name, budget_s=20.0):
     from oracle import pyoracle as po
 
     s = po.Sim(cfg, f["pos"], f["vel"], f["type"], mode=po.OR_REF_MIXED, use_cells=True)
-    step = s.step_nose_hoover if mode_name == "nh" else s.step_nve
+    if mode_name == "nh":
+        step = s.step_nose_hoover
+    elif mode_name == "nph":
+        step = lambda n: s.step_nph(1.0, n)  # noqa: E731
+    else:
+        step = s.step_nve
     t0 = time.perf_counter()
     n = 0
     while True:
@@ -132,11 +166,13 @@ def cpu_cell_baseline(f, cfg, mode_name, budget_s=20.0):
     dt = time.perf_counter() - t0
     return {"value": len(f) * n / dt, "unit": "particle-steps/s", "cores": os.cpu_count(),
             "kind": "port",
-            "sample": f"{n} full steps of the oracle's cell-list Nose-Hoover/NVE step "
+            "sample": f"{n} full steps of the oracle's cell-list "
+                      f"{dict(nh='Nose-Hoover', nph='NPH', nve='NVE')[mode_name]} step "
                       f"(reference mixed-precision pair arithmetic, OpenMP on all cores)"}
 
 
-def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=False):
+def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=False, shard=None,
+                     dist=None):
     """C4: the 512-system FIRE mix as ONE batch vs the same systems run one at
     a time through the single-system path (a stratified sample of
     `plain_sample` systems, each as a batch of one). particle-iterations are
@@ -150,6 +186,10 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
     S = wl.FIRE_SETTINGS
     params = wl.fire_params()
     systems = wl.fire_mix(512)
+    if shard is not None:  # this rank's systems (LPT by N, no collective on the data path)
+        rank, ws = shard
+        owner = lpt_assign([len(f) for f, _ in systems], ws)
+        systems = [x for x, r in zip(systems, owner) if r == rank]
     sizes = np.array([len(f) for f, _ in systems])
 
     def steps_of(b, ids):
@@ -163,9 +203,15 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
     s0 = steps_of(b, ids)
     t0 = time.perf_counter()
     b.run(-1 if to_completion else iters)
-    t_batch = time.perf_counter() - t0
+    t_batch = max_over_ranks(time.perf_counter() - t0, dist, dev)
     s1 = steps_of(b, ids)
     work = float((sizes * (s1 - s0)).sum())
+    if dist is not None:
+        import torch
+
+        tw = torch.tensor([work], device=dev, dtype=torch.float64)
+        dist.all_reduce(tw)
+        work = float(tw.item())
     done = int(b.progress()[1])
     converged = sum(1 for i in ids if b.system_info(i)[1] and b.system_info(i)[2] < S["max_steps"])
     del b
@@ -188,6 +234,7 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
     value = work / t_batch
     return {"metric": "particle-iterations/s", "value": value, "unit": "particle-iterations/s",
             "systems": len(systems), "particles": int(sizes.sum()),
+            "ranks": 1 if shard is None else shard[1],
             "window": ("to completion" if to_completion else f"iterations {warm_iters}.."
                        f"{warm_iters + iters}"),
             "seconds": t_batch, "build_and_warmup_s": t_build,
@@ -199,26 +246,42 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
 
 
 def run_fire_mix(args):
+    """The 512-system FIRE mix; with N ranks the systems are split by LPT on
+    their size, each rank runs its share as one batch, and the aggregate is
+    the total work over the slowest rank's time."""
     import torch
 
     ws, rank, local = _dist()
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(0)
-    clocks = ClockSampler(0)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local if ws > 1 else 0
+    torch.cuda.set_device(dev)
+    clocks = ClockSampler(dev)
     clocks.start()
-    res = measure_fire_mix(0, args.warmup, args.steps, to_completion=args.to_completion)
+    res = measure_fire_mix(dev, args.warmup, args.steps, to_completion=args.to_completion,
+                           shard=(rank, ws) if ws > 1 else None, dist=dist,
+                           plain_sample=32 // ws)
     clk = clocks.stop()
-    out = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": 1,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "fp32-pair/fp64-state",
-           "data": "synthetic (seeded uniform-random starts)",
-           "config": {"workload": "batched FIRE, 512 systems, N log-uniform [256, 16384], "
-                                  "f_A ~ U(0.2,0.8), rho ~ U(0.6,1.0), square periodic boxes, "
-                                  "uniform-random positions; dt_init 0.001, dt_max 0.01, "
-                                  "alpha0 0.1, f_inc 1.1, f_dec 0.5, tol 1e-6, 20000 its"},
-           "batched": res, "clocks": clk}
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        out = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": ws,
+               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+               "scaling": "strong", "vs_baseline": None, "dtype": "fp32-pair/fp64-state",
+               "data": "synthetic (seeded uniform-random starts)",
+               "config": {"workload": "batched FIRE, 512 systems, N log-uniform [256, 16384], "
+                                      "f_A ~ U(0.2,0.8), rho ~ U(0.6,1.0), square periodic "
+                                      "boxes, uniform-random positions; dt_init 0.001, dt_max "
+                                      "0.01, alpha0 0.1, f_inc 1.1, f_dec 0.5, tol 1e-6, 20000 "
+                                      "its", "parallelism": f"systems sharded by LPT over {ws}"},
+               "batched": res, "clocks": clk}
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
     return 0
 
 
@@ -373,8 +436,12 @@ def run_ours(args):
     f, cfg, mode, desc = make_workload(args.workload, rank)
     N = len(f)
     sim = mdb.MDSimulation(cfg, frame=f, device=dev)
-    step = (lambda n: sim.step_single_nose_hoover(nsteps=n)) if mode == "nh" else \
-        (lambda n: sim.step_single_NVE(nsteps=n))
+    if mode == "nh":
+        step = lambda n: sim.step_single_nose_hoover(nsteps=n)  # noqa: E731
+    elif mode == "nph":
+        step = lambda n: sim.step_single_NPH(1.0, nsteps=n)  # noqa: E731
+    else:
+        step = lambda n: sim.step_single_NVE(nsteps=n)  # noqa: E731
     stream = torch.cuda.ExternalStream(sim.cuda_stream(), device=dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     step(args.warmup)
@@ -407,18 +474,12 @@ def run_ours(args):
     o1 = sim.observables()
     launches = mdb.kernel_launches() - l0 + 10 * (o1.rebuilds - o0.rebuilds)
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t_local = t_ms / 1e3
-    if dist is not None:
-        t = torch.tensor([t_local], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    else:
-        t_max = t_local
+    t_max = max_over_ranks(t_ms / 1e3, dist, dev)
     value = N * ws * args.steps / t_max
 
     # ---- the dominant kernel: per-phase CUDA events on the launching stream --
     nph = 20
-    ms = sim.phase_times(nph, nose_hoover=(mode == "nh"))
+    ms = sim.phase_times(nph, nose_hoover=(mode == "nh"), nph=(mode == "nph"))
     t_force = ms[2] / nph / 1e3
     t_drift = ms[0] / nph / 1e3
     hbm_peak, peak_kind = _peaks()
@@ -454,11 +515,7 @@ def run_ours(args):
         step(1)
         _ = sim.observables()                # D2H of the step's result
     mdb._lib.check(mdb._lib.lib().mdb_sim_get_frame(sim._h, mdb._lib.frame_ptr(out_host), N))
-    e2e_t = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(time.perf_counter() - t0, dist, dev)
     e2e = {"value": N * ws * K2 / e2e_t, "unit": "particle-steps/s",
            "h2d_bytes_per_step": int(64 * N / K2) + 8,
            "d2h_bytes_per_step": int(64 * N / K2) + 112,
@@ -481,7 +538,10 @@ def run_ours(args):
             "dtype": "fp32-pair/fp64-state", "data": "synthetic (seeded jittered lattice)",
             "config": {"workload": desc, "N": N, "parallelism": f"replicas x{ws}",
                        "l2": "flushed between timed steps (256 MiB write outside the events)"},
-            "roofline": {"bound": "hbm", "kernel": "k_force<FM_NH> (pair force + NH kick + K)",
+            "roofline": {"bound": "hbm", "kernel": {
+                             "nh": "k_force<FM_NH> (pair force + NH kick + K)",
+                             "nph": "k_force<FM_NPH> (pair force + virial + kick + barostat)",
+                             "nve": "k_force<FM_NVE> (pair force + kick)"}[mode],
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "peak_source": peak_kind,
                          "traffic": traffic,
@@ -512,7 +572,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="nvt_slab",
-                    choices=["nvt_slab", "nve_4096", "fire_mix", "served"])
+                    choices=["nvt_slab", "nve_4096", "nph_4m", "fire_mix", "served"])
     ap.add_argument("--to-completion", action="store_true",
                     help="fire_mix: run every system until it converges or hits 20000 its")
     ap.add_argument("--requests", type=int, default=2000, help="served: number of requests")

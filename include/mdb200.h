@@ -213,7 +213,8 @@ int mdb_sim_save_pframe(mdb_sim_t* sim, const char* path, uint64_t frame_index);
 int mdb_sim_get_config(mdb_sim_t* sim, mdb_config_t* out);
 /* The cudaStream_t (as void*) all work of this handle is issued on. */
 int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream);
-/* Measurement aid: runs nsteps Nose-Hoover (kind 2) or NVE (kind 1) steps
+/* Measurement aid: runs nsteps Nose-Hoover (kind 2), NVE (kind 1) or NPH
+ * (kind 3, at the external pressure of the last mdb_sim_step_nph call) steps
  * with each phase launched separately and bracketed by CUDA events on the
  * handle's stream; ms_out[0..2] receive the summed drift, cell-rebuild and
  * force-phase times in milliseconds. The steps advance the simulation like

@@ -261,11 +261,13 @@ class MDSimulation:
     def synchronize(self) -> None:
         check(lib().mdb_sim_synchronize(self._h))
 
-    def phase_times(self, nsteps: int, nose_hoover: bool = True):
+    def phase_times(self, nsteps: int, nose_hoover: bool = True, nph: bool = False):
         """Summed (drift, rebuild, force) milliseconds of nsteps eager steps,
-        from CUDA events on this handle's stream."""
+        from CUDA events on this handle's stream (NPH steps at the pressure of
+        the last step_single_NPH call when nph is set)."""
         out = (C.c_double * 3)()
-        check(lib().mdb_sim_phase_times(self._h, 2 if nose_hoover else 1, int(nsteps), out))
+        kind = 3 if nph else (2 if nose_hoover else 1)
+        check(lib().mdb_sim_phase_times(self._h, kind, int(nsteps), out))
         return tuple(out)
 
     def cuda_stream(self) -> int:

@@ -321,9 +321,18 @@ int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream) {
 
 int mdb_sim_phase_times(mdb_sim_t* sim, int32_t kind, int64_t nsteps, double* ms_out) {
   if (!sim || !ms_out || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
-  if (kind != MDB_JOB_NVE && kind != MDB_JOB_NVT)
-    return mdb::set_error(MDB_ERR_ARG, "kind must be MDB_JOB_NVE or MDB_JOB_NVT");
+  if (kind != MDB_JOB_NVE && kind != MDB_JOB_NVT && kind != 3)
+    return mdb::set_error(MDB_ERR_ARG, "kind must be 1 (NVE), 2 (Nose-Hoover) or 3 (NPH)");
   MDB_TRY(leave_piston(sim));
+  if (kind == 3) {
+    if (!sim->nph_init || !sim->p_valid)
+      return mdb::set_error(MDB_ERR_STATE,
+                            "NPH phase times need a preceding mdb_sim_step_nph call");
+    MDB_TRY(sim->eng->run_md_timed(mdb::DM_NPH, mdb::FM_NPH, true, nsteps, ms_out));
+    sim->k_valid = false;
+    advance_time(sim, nsteps);
+    return MDB_OK;
+  }
   if (kind == MDB_JOB_NVT) {
     if (!sim->k_valid) MDB_TRY(sim->eng->reduce_K());
     MDB_TRY(sim->eng->run_md_timed(mdb::DM_NH, mdb::FM_NH, true, nsteps, ms_out));
