@@ -1154,8 +1154,10 @@ __global__ void k_rb_copyback(Dev D) {
 }
 
 // Verlet list of one slot: the 3x3 stencil candidates within the list radius
-// (rc_ij + skin), same displacement arithmetic as the force loop.
-template <bool PY>
+// (rc_ij + skin), same displacement arithmetic as the force loop. MIC = false
+// for interior cells (two or more cells from every periodic edge): the
+// stencil does not wrap, so the nearest image is the plain difference.
+template <bool PY, bool MIC>
 __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, const SysState& S,
                                           int64_t k, int& nowrap) {
   PairCtx c;
@@ -1209,7 +1211,7 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
         if (j == k) continue;
         const float4 q = D.pff[j];
         float dx, dy;
-        const float r2 = pair_r2<PY>(q, c, dx, dy);
+        const float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
         const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
         const float rl2 = (tj == ts) ? rl2s : rl2ab;
         if (r2 < rl2) {
@@ -1249,14 +1251,6 @@ __global__ void k_rb_nlist(Dev D) {
       D.ncount[k] = -1;
       continue;
     }
-    int nowrap = 0;
-    const int cnt = S->periodic_y ? build_list<true>(D, P, *S, k, nowrap)
-                                  : build_list<false>(D, P, *S, k, nowrap);
-    if (cnt > D.max_nbr) {
-      D.ncount[k] = -1;  // too many neighbours: the force loop scans the stencil
-      atomicAdd(&S->nl_overflow, 1);
-      continue;
-    }
     // Interior build cells (two or more cells from each periodic edge) with
     // unwrapped offsets: the partners were binned one cell away at most and
     // move less than half a cell before the next rebuild, so no pair needs
@@ -1265,6 +1259,19 @@ __global__ void k_rb_nlist(Dev D) {
     const int cx = cell % S->ncx, cy = cell / S->ncx;
     const bool interior = cx >= 2 && cx <= S->ncx - 3 &&
                           (!S->periodic_y || (cy >= 2 && cy <= S->ncy - 3));
+    int nowrap = 0;
+    int cnt;
+    if (S->periodic_y)
+      cnt = interior ? build_list<true, false>(D, P, *S, k, nowrap)
+                     : build_list<true, true>(D, P, *S, k, nowrap);
+    else
+      cnt = interior ? build_list<false, false>(D, P, *S, k, nowrap)
+                     : build_list<false, true>(D, P, *S, k, nowrap);
+    if (cnt > D.max_nbr) {
+      D.ncount[k] = -1;  // too many neighbours: the force loop scans the stencil
+      atomicAdd(&S->nl_overflow, 1);
+      continue;
+    }
     D.ncount[k] = cnt | ((interior && nowrap) ? kListInterior : 0);
   }
 }
