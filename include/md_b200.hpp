@@ -274,6 +274,12 @@ class MDSimulation {
 
   double cal_total_K() { return scalar(mdb_sim_total_K, "cal_total_K"); }
   double cal_total_U() { return scalar(mdb_sim_total_U, "cal_total_U"); }
+  // cal_partial_U_lambda (src/md_env.cu:2362-2406)
+  double cal_partial_U_lambda(double epsilon_lambda) {
+    double v = 0.0;
+    check(mdb_sim_partial_U_lambda(sim_, epsilon_lambda, &v), "cal_partial_U_lambda");
+    return v;
+  }
   double cal_instant_pressure() {
     return scalar(mdb_sim_instant_pressure, "cal_instant_pressure");
   }

@@ -182,6 +182,12 @@ int mdb_sim_step_nph_piston(mdb_sim_t* sim, double p_ext, int64_t nsteps);
 int mdb_sim_total_K(mdb_sim_t* sim, double* out);
 /* cal_total_U (src/md_env.cu:2347-2360), including wall energy in piston mode. */
 int mdb_sim_total_U(mdb_sim_t* sim, double* out);
+/* cal_partial_U_lambda (src/md_env.cu:2362-2406, kernel
+ * src/md_cuda_common.cu:266-377): -epsilon_lambda * 1/2 sum_i sum_j
+ * (Fx dx - Fy dy) over the current frame (FP32 pair force, FP64 products and
+ * sums), y periodic unless the piston mode is active. The reference counts
+ * x-edge partners twice at MPI world size 1; this is the nearest-image sum. */
+int mdb_sim_partial_U_lambda(mdb_sim_t* sim, double epsilon_lambda, double* out);
 /* cal_instant_pressure (src/md_env.cu:2254-2266). */
 int mdb_sim_instant_pressure(mdb_sim_t* sim, double* out);
 
@@ -304,6 +310,10 @@ int mdb_batch_energies_all(mdb_batch_t* b, double* K, double* U, double* xi, int
 int mdb_batch_issue(mdb_batch_t* b, int64_t iterations, int64_t* issued);
 int mdb_batch_query(mdb_batch_t* b, int32_t* idle);
 int mdb_batch_collect(mdb_batch_t* b);
+/* mdb_sim_partial_U_lambda for every system of a batch (n = number of
+ * systems), e.g. the points of a lambda sweep run as one batch. */
+int mdb_batch_partial_U_lambda_all(mdb_batch_t* b, double epsilon_lambda, double* out,
+                                   int32_t n);
 /* Which systems have finished, as of the last run or collect (n = number of
  * systems). */
 int mdb_batch_done_flags(mdb_batch_t* b, int32_t* done, int32_t n);

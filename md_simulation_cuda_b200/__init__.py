@@ -202,6 +202,13 @@ class MDSimulation:
     def cal_total_U(self) -> float:
         return self._scalar(lib().mdb_sim_total_U)
 
+    def cal_partial_U_lambda(self, epsilon_lambda: float) -> float:
+        """dU/dlambda of the area-preserving deformation (MDSimulation::
+        cal_partial_U_lambda, src/md_env.cu:2362-2406)."""
+        v = C.c_double()
+        check(lib().mdb_sim_partial_U_lambda(self._h, float(epsilon_lambda), C.byref(v)))
+        return v.value
+
     def cal_instant_pressure(self) -> float:
         return self._scalar(lib().mdb_sim_instant_pressure)
 
@@ -453,6 +460,14 @@ class Batch:
         d = np.zeros(len(self._sizes), dtype=np.int32)
         check(lib().mdb_batch_done_flags(self._h, d.ctypes.data_as(C.POINTER(C.c_int32)), len(d)))
         return d.astype(bool)
+
+    def partial_U_lambda(self, epsilon_lambda: float) -> np.ndarray:
+        """cal_partial_U_lambda of every system."""
+        out = np.zeros(len(self._sizes))
+        check(lib().mdb_batch_partial_U_lambda_all(self._h, float(epsilon_lambda),
+                                                   out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                   len(out)))
+        return out
 
     def energies(self, sys_id: int):
         """(K, U, xi) of one system."""

@@ -229,6 +229,7 @@ SIGNATURES = {
     "mdb_sim_total_K": ([_vp, _dp], C.c_int),
     "mdb_sim_total_U": ([_vp, _dp], C.c_int),
     "mdb_sim_instant_pressure": ([_vp, _dp], C.c_int),
+    "mdb_sim_partial_U_lambda": ([_vp, C.c_double, _dp], C.c_int),
     "mdb_sim_observables": ([_vp, C.POINTER(MDBObservables)], C.c_int),
     "mdb_sim_get_frame": ([_vp, _vp, C.c_int64], C.c_int),
     "mdb_sim_set_frame": ([_vp, _vp, C.c_int64], C.c_int),
@@ -256,6 +257,7 @@ SIGNATURES = {
     "mdb_batch_query": ([_vp, _ip], C.c_int),
     "mdb_batch_collect": ([_vp], C.c_int),
     "mdb_batch_done_flags": ([_vp, _ip, C.c_int32], C.c_int),
+    "mdb_batch_partial_U_lambda_all": ([_vp, C.c_double, _dp, C.c_int32], C.c_int),
     "mdb_batch_device_bytes": ([_vp, C.POINTER(C.c_int64)], C.c_int),
     "mdb_batch_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
     "mdb_server_options_default": ([C.POINTER(MDBServerOptions)], None),

@@ -234,6 +234,16 @@ int mdb_sim_total_U(mdb_sim_t* sim, double* out) {
   return check_status(sim);
 }
 
+int mdb_sim_partial_U_lambda(mdb_sim_t* sim, double epsilon_lambda, double* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  // periodic_y = piston_mode_active ? 0 : 1 (src/md_env.cu:2369)
+  MDB_TRY(sim->eng->force(mdb::FM_OBS, !sim->piston_active));
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  *out = -epsilon_lambda * S.Wani;
+  return check_status(sim);
+}
+
 int mdb_sim_instant_pressure(mdb_sim_t* sim, double* out) {
   if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
   MDB_TRY(sim->eng->force(mdb::FM_OBS, !sim->piston_active));
@@ -701,6 +711,17 @@ int mdb_batch_energies(mdb_batch_t* b, int32_t sys_id, double* K, double* U, dou
   if (U) *U = S[sys_id].U;
   if (xi) *xi = S[sys_id].xi;
   if (S[sys_id].nonfinite) return mdb::set_error(MDB_ERR_NONFINITE, "non-finite state");
+  return MDB_OK;
+}
+
+int mdb_batch_partial_U_lambda_all(mdb_batch_t* b, double epsilon_lambda, double* out,
+                                   int32_t n) {
+  if (!b || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (n != b->eng->nsys()) return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the number of systems");
+  std::vector<SysState> S;
+  MDB_TRY(obs_energies(*b->eng, S));
+  for (int32_t s = 0; s < n; ++s) out[s] = -epsilon_lambda * S[s].Wani;
   return MDB_OK;
 }
 

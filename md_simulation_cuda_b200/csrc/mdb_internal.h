@@ -76,6 +76,7 @@ struct SysState {
   double fl, ce;                      // Ly clamp bounds
   double vp, Fp, wallU;               // piston
   double U, Wv, kin, kin2;            // last observable reductions
+  double Wani;                        // 1/2 sum (Fx dx - Fy dy) of the last observation
   double p_ext;                       // external pressure of the running call
   double inv_wx, inv_wy, Lx_b, Ly_b;  // cell grid at the last rebuild
   int32_t ncx, ncy, allpairs, periodic_y;

@@ -210,7 +210,7 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
 // Number of sums / maxima each phase reduces.
 template <int FM>
 struct ForceRed {
-  static constexpr int NS = (FM == FM_OBS) ? 5 : (FM == FM_NPH) ? 3
+  static constexpr int NS = (FM == FM_OBS) ? 6 : (FM == FM_NPH) ? 3
                           : (FM == FM_INIT || FM == FM_PISTON) ? 2
                           : (FM == FM_NH || FM == FM_FIRE) ? 1 : 0;
   static constexpr int NM = (FM == FM_FIRE) ? 2 : 0;
@@ -285,7 +285,7 @@ __device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float
 template <bool PY, bool ENERGY, bool VIRIAL, bool MIC = true>
 __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float& fxs, float& fxc,
                                          float& fys, float& fyc, float& ws, float& wc,
-                                         double& u) {
+                                         double& u, double& an) {
   float dx, dy;
   const float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
   const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
@@ -307,6 +307,9 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
       const float e4 = same ? c.e4s : c.e4ab;
       const double vc = same ? c.Vcs : c.Vcab;
       u = fma(0.5, (double)(e4 * (sr12 - sr6)) - vc, u);
+      // Fx dx - Fy dy of cal_partial_U_lambda_kernel (src/md_cuda_common.cu:
+      // 345-355): products of FP32 values, exact in FP64
+      an += (double)(tmp * dx) * (double)dx - (double)(tmp * dy) * (double)dy;
     }
   }
 }
@@ -323,7 +326,7 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
                                           int li, int n, int nn, const PairCtx& c, float& fxs,
                                           float& fxc, float& fys, float& fyc, float& ws,
-                                          float& wc, double& u) {
+                                          float& wc, double& u, double& an) {
   const IDX* __restrict__ p = nlist + i;
   // MIC: slot 0 of the system and a wrapped index; interior: slot i itself
   const float4* __restrict__ base = MIC ? pff + (i - li) : pff + i;
@@ -343,7 +346,7 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
     }
 #pragma unroll
     for (int q = 0; q < PF; ++q)
-      pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u);
+      pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u, an);
   }
   for (; k < nn; ++k) {
     int t = (int)__ldg(p + (int64_t)k * ntot);
@@ -352,7 +355,7 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
       t += (t < 0) ? n : 0;
       t -= (t >= n) ? n : 0;
     }
-    pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u);
+    pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u, an);
   }
 }
 
@@ -360,9 +363,10 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
 template <bool PY, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
                                            const PairCtx& c, float& fxs, float& fxc, float& fys,
-                                           float& fyc, float& ws, float& wc, double& u) {
+                                           float& fyc, float& ws, float& wc, double& u,
+                                           double& an) {
 #pragma unroll 4
-  for (int j = j0; j < j1; ++j) pair_one<PY, ENERGY, VIRIAL>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u);
+  for (int j = j0; j < j1; ++j) pair_one<PY, ENERGY, VIRIAL>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u, an);
 }
 
 __device__ __forceinline__ void split_box(double L, float& h, float& l, float& inv) {
@@ -376,7 +380,8 @@ __device__ __forceinline__ void split_box(double L, float& h, float& l, float& i
 template <bool PY, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
                                                int64_t i, int ti, double Lx, double Ly,
-                                               double& fx, double& fy, double& w, double& u) {
+                                               double& fx, double& fy, double& w, double& u,
+                                               double& an) {
   PairCtx c;
   const float4 qi = __ldg(D.pff + i);
   c.xih = fabsf(qi.x);
@@ -400,6 +405,7 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   c.Vcab = P.Vc[2];
   float fxs = 0.f, fxc = 0.f, fys = 0.f, fyc = 0.f, ws = 0.f, wc = 0.f;
   u = 0.0;
+  an = 0.0;
   const float4* __restrict__ pff = D.pff;
   const int nc = __ldg(D.ncount + i);
   if (nc >= 0) {
@@ -408,21 +414,21 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
     if (D.nl16) {
       if (nc & kListInterior)
         pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                             fys, fyc, ws, wc, u);
+                                             fys, fyc, ws, wc, u, an);
       else
         pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                            fys, fyc, ws, wc, u);
+                                            fys, fyc, ws, wc, u, an);
     } else {
       if (nc & kListInterior)
         pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                             fys, fyc, ws, wc, u);
+                                             fys, fyc, ws, wc, u, an);
       else
         pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                            fys, fyc, ws, wc, u);
+                                            fys, fyc, ws, wc, u, an);
     }
   } else if (S.allpairs) {
     pair_range<PY, ENERGY, VIRIAL>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
-                                   wc, u);
+                                   wc, u, an);
   } else {
     const int ncx = S.ncx, ncy = S.ncy;
     const int cell = D.cell_of[i];
@@ -440,17 +446,17 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
       const int64_t row = P.c0 + (int64_t)yy * ncx;
       if (cx > 0 && cx < ncx - 1) {
         pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + cx - 1), __ldg(cs + row + cx + 2), c,
-                                       fxs, fxc, fys, fyc, ws, wc, u);
+                                       fxs, fxc, fys, fyc, ws, wc, u, an);
       } else if (cx == 0) {
         pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fxs, fxc, fys,
-                                       fyc, ws, wc, u);
+                                       fyc, ws, wc, u, an);
         pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 1), __ldg(cs + row + ncx), c,
-                                       fxs, fxc, fys, fyc, ws, wc, u);
+                                       fxs, fxc, fys, fyc, ws, wc, u, an);
       } else {
         pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 2), __ldg(cs + row + ncx), c,
-                                       fxs, fxc, fys, fyc, ws, wc, u);
+                                       fxs, fxc, fys, fyc, ws, wc, u, an);
         pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fxs, fxc,
-                                       fys, fyc, ws, wc, u);
+                                       fys, fyc, ws, wc, u, an);
       }
     }
   }
@@ -516,8 +522,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
     const int64_t i = base + (int64_t)it * kThreads;
     if (skip || i >= end) break;
     const int ti = D.type[i];
-    double fx, fy, w, u;
-    particle_force<PY, kEnergy, kVirial>(D, P, *S, i, ti, Lx, Ly, fx, fy, w, u);
+    double fx, fy, w, u, an;
+    particle_force<PY, kEnergy, kVirial>(D, P, *S, i, ti, Lx, Ly, fx, fy, w, u, an);
     const double m = type_mass(P, ti);
     double2 v = D.vel[i];
     if (FM == FM_OBS) {
@@ -530,6 +536,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
         red[3] += up;
         red[4] += en;
       }
+      red[5] += an;
     } else {
       double ax = fx / m, ay = fy / m;
       if (!PY && (FM == FM_INIT || FM == FM_PISTON)) {
@@ -612,6 +619,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       S->kin = tot[2];
       S->kin2 = tot[3];
       S->wallU = tot[4];
+      S->Wani = 0.5 * tot[5];
     } else if (FM == FM_FIRE) {
       // FIRE control (src/md_energy_minimizer.cu:171-203)
       const double maxf = (tmx[1] > 0.0) ? __longlong_as_double(0x7ff8000000000000ULL) : tmx[0];

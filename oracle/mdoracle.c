@@ -433,6 +433,69 @@ int64_t or_count_pairs(const or_lj_t* lj, int64_t n, const double* pos, const in
   return total;
 }
 
+/* cal_partial_U_lambda_kernel (src/md_cuda_common.cu:266-377) and its host
+ * sum (src/md_env.cu:2362-2406), all pairs with the nearest image (no halo
+ * duplication): sum over ordered pairs of 1/2 * (-eps_lambda) * (Fx dx - Fy dy).
+ * OR_REF_MIXED: FP32 pair force, products and sum in FP64 as the kernel does;
+ * OR_FP64: every operation in double. *scale receives the same sum with
+ * |Fx dx| + |Fy dy| (a magnitude for tolerances). */
+int or_partial_U_lambda(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
+                        double Lx, double Ly, int32_t periodic_y, int32_t mode,
+                        double epsilon_lambda, double* out, double* scale, int32_t nthreads) {
+  if (!lj || !pos || !type || !out || n < 0) return 1;
+  set_threads(nthreads);
+  const float Lx_f = (float)Lx, Ly_f = (float)Ly;
+  double total = 0.0, mag = 0.0;
+#pragma omp parallel for reduction(+ : total, mag) schedule(dynamic, 16)
+  for (int64_t i = 0; i < n; ++i) {
+    double ui = 0.0, mi = 0.0;
+    for (int64_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const int c = pair_class(type[i], type[j]);
+      double fxdx, fydy;
+      if (mode == OR_FP64) {
+        double dx = pos[2 * i] - pos[2 * j];
+        double dy = pos[2 * i + 1] - pos[2 * j + 1];
+        dx = dx - Lx * round(dx / Lx);
+        if (periodic_y) dy = dy - Ly * round(dy / Ly);
+        const double sig = lj->sigma[c], rc = lj->cutoff * sig;
+        const double r2 = dx * dx + dy * dy;
+        if (!(r2 > 0.0 && r2 < rc * rc)) continue;
+        const double r2i = 1.0 / r2;
+        const double sr2 = sig * sig * r2i;
+        const double sr6 = sr2 * sr2 * sr2;
+        const double sr12 = sr6 * sr6;
+        const double tmp = 24.0 * lj->epsilon[c] * (2.0 * sr12 - sr6) * r2i;
+        fxdx = (tmp * dx) * dx;
+        fydy = (tmp * dy) * dy;
+      } else {
+        float dx_f = (float)(pos[2 * i] - pos[2 * j]);
+        float dy_f = (float)(pos[2 * i + 1] - pos[2 * j + 1]);
+        dx_f = fmaf(-Lx_f, roundf(dx_f / Lx_f), dx_f);
+        if (periodic_y) dy_f = fmaf(-Ly_f, roundf(dy_f / Ly_f), dy_f);
+        const float sigma_f = (float)lj->sigma[c];
+        const float rc_f = (float)lj->cutoff * sigma_f;
+        const float dr_sq_f = fmaf(dx_f, dx_f, dy_f * dy_f);
+        if (!(dr_sq_f > 0.0f && dr_sq_f < rc_f * rc_f)) continue;
+        const float r2_inv_f = 1.0f / dr_sq_f;
+        const float sr2_f = (sigma_f * sigma_f) * r2_inv_f;
+        const float sr6_f = sr2_f * sr2_f * sr2_f;
+        const float sr12_f = sr6_f * sr6_f;
+        const float tmp_f = (24.0f * (float)lj->epsilon[c]) * fmaf(2.0f, sr12_f, -sr6_f) * r2_inv_f;
+        fxdx = (double)(tmp_f * dx_f) * (double)dx_f;
+        fydy = (double)(tmp_f * dy_f) * (double)dy_f;
+      }
+      ui += 0.5 * (-epsilon_lambda * (fxdx - fydy));
+      mi += 0.5 * fabs(epsilon_lambda) * (fabs(fxdx) + fabs(fydy));
+    }
+    total += ui;
+    mag += mi;
+  }
+  *out = total;
+  if (scale) *scale = mag;
+  return 0;
+}
+
 /* ---- engine --------------------------------------------------------------- */
 static void sim_forces(or_sim_t* s, int32_t periodic_y, double* acc, double* U, double* W) {
   if (s->use_cells && !s->ws1_halo)

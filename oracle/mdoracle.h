@@ -67,6 +67,13 @@ int or_forces_cells(const or_lj_t* lj, int64_t n, const double* pos, const int32
 int or_forces_rows(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
                    double Lx, double Ly, int32_t periodic_y, int32_t mode, int64_t row0,
                    int64_t nrows, double* acc_rows, int32_t nthreads);
+/* MDSimulation::cal_partial_U_lambda (src/md_env.cu:2362-2406, kernel
+ * src/md_cuda_common.cu:266-377) with the nearest image: out = sum over
+ * ordered pairs of 1/2 * (-eps_lambda) * (Fx dx - Fy dy); scale (optional) =
+ * the same sum of magnitudes. */
+int or_partial_U_lambda(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
+                        double Lx, double Ly, int32_t periodic_y, int32_t mode,
+                        double epsilon_lambda, double* out, double* scale, int32_t nthreads);
 /* Ordered in-cutoff pairs counted through a cell list (large systems). */
 int64_t or_count_pairs_cells(const or_lj_t* lj, int64_t n, const double* pos,
                              const int32_t* type, double Lx, double Ly, int32_t nthreads);

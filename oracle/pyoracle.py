@@ -117,6 +117,9 @@ def lib():
             L.or_count_pairs.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
                                          C.c_double, C.c_int32, C.c_int32]
             L.or_count_pairs.restype = C.c_int64
+            L.or_partial_U_lambda.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
+                                              C.c_double, C.c_int32, C.c_int32, C.c_double, dp,
+                                              dp, C.c_int32]
             L.or_count_pairs_cells.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
                                                C.c_double, C.c_int32]
             L.or_count_pairs_cells.restype = C.c_int64
@@ -200,6 +203,20 @@ def count_pairs(cfg, pos, types, Lx, Ly, periodic_y=1, nthreads=0):
     lj = make_lj(cfg)
     return int(lib().or_count_pairs(C.byref(lj), p.shape[0], _dp(p), _ip(t), Lx, Ly, periodic_y,
                                     nthreads))
+
+
+def partial_U_lambda(cfg, pos, types, Lx, Ly, eps_lambda, periodic_y=1, mode=0, nthreads=0):
+    """(dU/dlambda, magnitude scale) of or_partial_U_lambda (all pairs)."""
+    p = _pos2(pos)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    lj = make_lj(cfg)
+    out = C.c_double()
+    scale = C.c_double()
+    rc = lib().or_partial_U_lambda(C.byref(lj), p.shape[0], _dp(p), _ip(t), Lx, Ly, periodic_y,
+                                   mode, float(eps_lambda), C.byref(out), C.byref(scale),
+                                   nthreads)
+    assert rc == 0
+    return out.value, scale.value
 
 
 def count_pairs_cells(cfg, pos, types, Lx, Ly, nthreads=0):

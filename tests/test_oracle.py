@@ -142,3 +142,25 @@ def test_nh_thermostat_holds_temperature():
         s.step_nose_hoover(10)
         ts.append(2 * s.total_K() / (2 * 400 - 2))
     assert abs(np.mean(ts[50:]) - 0.8) < 0.08
+
+
+def test_partial_U_lambda_two_particles():
+    """dU/dlambda of the area-preserving stretch: a pair along x contributes
+    -eps_lambda * tmp * r^2 (both ordered pairs, each halved), along y the
+    opposite sign (src/md_cuda_common.cu:345-355)."""
+    from md_simulation_cuda_b200 import workloads as wl
+
+    cfg = wl.config_dict(2, 10.0, 10.0, dt=0.001, SIGMA_BB=1.0, SIGMA_AB=1.0, EPSILON_BB=1.0,
+                         EPSILON_AB=1.0)
+    for r in (0.97, 1.1, 1.5, 2.3):
+        tmp = 24 * (2 * r ** -14 - r ** -8)
+        for mode in (po.OR_FP64, po.OR_REF_MIXED):
+            vx, _ = po.partial_U_lambda(cfg, np.array([[9.8, 5.0], [(9.8 + r) % 10, 5.0]]),
+                                        [0, 0], 10.0, 10.0, 0.01, mode=mode)
+            vy, _ = po.partial_U_lambda(cfg, np.array([[5.0, 1.0], [5.0, 1.0 + r]]), [0, 0],
+                                        10.0, 10.0, 0.01, mode=mode)
+            # the mixed mode casts the unwrapped FP64 difference across the
+            # periodic edge to FP32 (the reference's own error, ~2e-5 here)
+            tol = 1e-12 if mode == po.OR_FP64 else 1e-4
+            assert abs(vx + 0.01 * tmp * r * r) <= tol * abs(tmp * r * r) * 0.01 + 1e-14
+            assert abs(vy - 0.01 * tmp * r * r) <= tol * abs(tmp * r * r) * 0.01 + 1e-14
