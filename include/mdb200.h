@@ -216,6 +216,19 @@ int mdb_sim_set_frame(mdb_sim_t* sim, const mdb_particle_t* frame, int64_t n);
 /* save_env (src/md_env.cu:4106-4124): appends the current frame to a PFRAME
  * file (created when absent). */
 int mdb_sim_save_pframe(mdb_sim_t* sim, const char* path, uint64_t frame_index);
+/* Checkpoint: save_env's PFRAME frame (appended to frame_path) plus a state
+ * file (JSON text) with what the reference's restart from a frame loses
+ * (MDSimulation(cfg, comm, file, step), src/md_env.cu:81-164, restarts with
+ * the configuration's box, xi = 0 and fresh barostat / piston state): t, the
+ * box, xi, K, p_A, the aspect ratio and Ly clamps, the piston velocity and
+ * force, the external pressure and the mode flags. Restoring builds the
+ * simulation from the frame with the saved box and state, so the following
+ * steps continue the saved trajectory. */
+int mdb_sim_save_checkpoint(mdb_sim_t* sim, const char* frame_path, uint64_t frame_index,
+                            const char* state_path);
+int mdb_sim_create_from_checkpoint(const mdb_config_t* cfg, const char* frame_path,
+                                   uint64_t frame_index, const char* state_path,
+                                   const mdb_options_t* opt, mdb_sim_t** out);
 int mdb_sim_get_config(mdb_sim_t* sim, mdb_config_t* out);
 /* The cudaStream_t (as void*) all work of this handle is issued on. */
 int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream);
@@ -228,6 +241,23 @@ int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream);
 int mdb_sim_phase_times(mdb_sim_t* sim, int32_t kind, int64_t nsteps, double* ms_out);
 /* Block until all issued work of the handle has finished. */
 int mdb_sim_synchronize(mdb_sim_t* sim);
+
+/* ---- asynchronous trajectory writer ---------------------------------------
+ * save_env (src/md_env.cu:4106-4124) writes a PFRAME frame and returns when it
+ * is on disk. mdb_traj_writer_write instead queues the export of the
+ * simulation's current frame on the simulation's stream (after the steps
+ * issued so far) into one of `depth` pinned staging slots and returns; a
+ * writer thread compresses and appends each frame to `path` (created unless
+ * append != 0) in the same PFRAME v2 format. A write waits only when all
+ * slots are in flight. flush waits until every queued frame is on disk; close
+ * flushes, stops the thread and frees the slots. Both return the first I/O or
+ * CUDA error of any queued frame. */
+typedef struct mdb_traj_writer mdb_traj_writer_t;
+int mdb_traj_writer_open(const char* path, int32_t append, int32_t depth,
+                         mdb_traj_writer_t** out);
+int mdb_traj_writer_write(mdb_traj_writer_t* w, mdb_sim_t* sim, uint64_t frame_index);
+int mdb_traj_writer_flush(mdb_traj_writer_t* w);
+int mdb_traj_writer_close(mdb_traj_writer_t* w);
 
 /* ---- FIRE minimiser (class EnergyMinimizer, include/md_energy_minimizer.hpp)
  */

@@ -145,13 +145,19 @@ class MDSimulation:
 
     def __init__(self, config_manager, comm=None, filename: Optional[str] = None,
                  step: Optional[int] = None, *, frame=None, device: int = 0,
-                 skin: Optional[float] = None, use_graphs: bool = True):
+                 skin: Optional[float] = None, use_graphs: bool = True,
+                 state_file: Optional[str] = None):
         self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
             else MDConfigManager(_config_of(config_manager))
         self._h = C.c_void_p()
         opt = options(device, skin, use_graphs)
         cfg = self.cfg_manager.config
-        if filename is not None:
+        if state_file is not None:
+            # a checkpoint: frame `step` of `filename` plus the integrator state
+            check(lib().mdb_sim_create_from_checkpoint(
+                C.byref(cfg), os.fsencode(filename), int(step or 0), os.fsencode(state_file),
+                C.byref(opt), C.byref(self._h)))
+        elif filename is not None:
             check(lib().mdb_sim_create_from_pframe(C.byref(cfg), os.fsencode(filename),
                                                    int(step or 0), C.byref(opt),
                                                    C.byref(self._h)))
@@ -261,6 +267,12 @@ class MDSimulation:
     def set_frame(self, frame) -> None:
         f = _as_frame(frame)
         check(lib().mdb_sim_set_frame(self._h, frame_ptr(f), len(f)))
+
+    def save_checkpoint(self, filename: str, step: int, state_file: str) -> None:
+        """save_env plus the integrator state (restore with
+        MDSimulation(cfg, filename=..., step=..., state_file=...))."""
+        check(lib().mdb_sim_save_checkpoint(self._h, os.fsencode(filename), int(step),
+                                            os.fsencode(state_file)))
 
     def save_env(self, filename: str, step: int) -> None:
         check(lib().mdb_sim_save_pframe(self._h, os.fsencode(filename), int(step)))
@@ -374,6 +386,39 @@ class FileWriter:
         check(lib().mdb_pframe_write(os.fsencode(self.path), 0 if self._fresh else 1,
                                      frame_ptr(f), len(f), int(frame_index)))
         self._fresh = False
+
+
+class TrajectoryWriter:
+    """Asynchronous PFRAME writer (mdb_traj_writer_*): write() queues the
+    simulation's current frame and returns; a thread compresses and appends."""
+
+    def __init__(self, path: str, append: bool = False, depth: int = 4):
+        self._h = C.c_void_p()
+        check(lib().mdb_traj_writer_open(os.fsencode(path), 1 if append else 0, int(depth),
+                                         C.byref(self._h)))
+
+    def write(self, sim: "MDSimulation", frame_index: int) -> None:
+        check(lib().mdb_traj_writer_write(self._h, sim._h, int(frame_index)))
+
+    def flush(self) -> None:
+        check(lib().mdb_traj_writer_flush(self._h))
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            h, self._h = self._h, C.c_void_p()
+            check(lib().mdb_traj_writer_close(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class FileReader:

@@ -235,6 +235,13 @@ SIGNATURES = {
     "mdb_sim_set_frame": ([_vp, _vp, C.c_int64], C.c_int),
     "mdb_sim_save_pframe": ([_vp, C.c_char_p, C.c_uint64], C.c_int),
     "mdb_sim_get_config": ([_vp, _cfgp], C.c_int),
+    "mdb_sim_save_checkpoint": ([_vp, C.c_char_p, C.c_uint64, C.c_char_p], C.c_int),
+    "mdb_sim_create_from_checkpoint": ([_cfgp, C.c_char_p, C.c_uint64, C.c_char_p, _optp,
+                                        C.POINTER(_vp)], C.c_int),
+    "mdb_traj_writer_open": ([C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp)], C.c_int),
+    "mdb_traj_writer_write": ([_vp, _vp, C.c_uint64], C.c_int),
+    "mdb_traj_writer_flush": ([_vp], C.c_int),
+    "mdb_traj_writer_close": ([_vp], C.c_int),
     "mdb_sim_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
     "mdb_sim_synchronize": ([_vp], C.c_int),
     "mdb_sim_phase_times": ([_vp, C.c_int32, C.c_int64, _dp], C.c_int),

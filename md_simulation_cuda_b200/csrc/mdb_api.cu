@@ -90,6 +90,20 @@ void advance_time(mdb_sim_t* sim, int64_t n) {
 
 }  // namespace
 
+namespace mdb {
+
+int sim_export_async(mdb_sim_t* sim, mdb_particle_t* host, cudaEvent_t ev) {
+  MDB_TRY(sim->eng->export_async(0, host));
+  MDB_CUDA(cudaEventRecord(ev, sim->eng->stream()));
+  return MDB_OK;
+}
+
+int64_t sim_particles(mdb_sim_t* sim) { return sim->eng->n(0); }
+
+int sim_device(mdb_sim_t* sim) { return sim->eng->device(); }
+
+}  // namespace mdb
+
 extern "C" {
 
 int mdb_sim_create(const mdb_config_t* cfg, const mdb_particle_t* frame, int64_t n,
@@ -311,6 +325,143 @@ int mdb_sim_save_pframe(mdb_sim_t* sim, const char* path, uint64_t frame_index) 
   int rc = mdb_pframe_write(path, 1, f.data(), (int64_t)f.size(), frame_index);
   if (rc != MDB_OK) rc = mdb_pframe_write(path, 0, f.data(), (int64_t)f.size(), frame_index);
   return rc;
+}
+
+namespace {
+
+// Integrator state beside a PFRAME frame: one "key": value per line.
+struct Checkpoint {
+  uint64_t frame_index = 0;
+  int64_t n = 0, steps = 0;
+  double t = 0, Lx = 0, Ly = 0, xi = 0, K = 0, pA = 0, aspect = 0, P_cur = 0, last_P = 0;
+  double fl = 0, ce = 0, vp = 0, Fp = 0, wallU = 0, p_ext = 0;
+  int clamped = 0, piston_active = 0, nph_init = 0, vp_init = 0, k_valid = 0, p_valid = 0;
+  int periodic_y = 1;
+};
+
+const char* kCheckpointFormat = "mdb200-checkpoint-1";
+
+bool ck_find(const std::string& text, const char* key, double* out) {
+  const std::string pat = std::string("\"") + key + "\":";
+  const size_t at = text.find(pat);
+  if (at == std::string::npos) return false;
+  const char* p = text.c_str() + at + pat.size();
+  char* end = nullptr;
+  const double v = strtod(p, &end);
+  if (end == p) return false;
+  *out = v;
+  return true;
+}
+
+}  // namespace
+
+int mdb_sim_save_checkpoint(mdb_sim_t* sim, const char* frame_path, uint64_t frame_index,
+                            const char* state_path) {
+  if (!sim || !frame_path || !state_path) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(mdb_sim_save_pframe(sim, frame_path, frame_index));
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  FILE* f = fopen(state_path, "wb");
+  if (!f) return mdb::set_error(MDB_ERR_IO, std::string("cannot open ") + state_path);
+  fprintf(f, "{\n  \"format\": \"%s\",\n", kCheckpointFormat);
+  fprintf(f, "  \"frame_index\": %llu,\n  \"n\": %lld,\n  \"steps\": %lld,\n",
+          (unsigned long long)frame_index, (long long)sim->eng->n(0), (long long)S.steps);
+  const struct {
+    const char* k;
+    double v;
+  } dv[] = {{"t", sim->t},     {"Lx", S.Lx},         {"Ly", S.Ly},         {"xi", S.xi},
+            {"K", S.K},        {"pA", S.pA},         {"aspect", S.aspect}, {"P_cur", S.P_cur},
+            {"last_P", S.last_P}, {"fl", S.fl},      {"ce", S.ce},         {"vp", S.vp},
+            {"Fp", S.Fp},      {"wallU", S.wallU},   {"p_ext", S.p_ext}};
+  for (const auto& e : dv) fprintf(f, "  \"%s\": %.17g,\n", e.k, e.v);
+  fprintf(f,
+          "  \"clamped\": %d,\n  \"piston_active\": %d,\n  \"nph_init\": %d,\n"
+          "  \"vp_init\": %d,\n  \"k_valid\": %d,\n  \"p_valid\": %d,\n  \"periodic_y\": %d\n}\n",
+          S.clamped, sim->piston_active ? 1 : 0, sim->nph_init ? 1 : 0, sim->vp_init ? 1 : 0,
+          sim->k_valid ? 1 : 0, sim->p_valid ? 1 : 0, sim->periodic_y);
+  if (fclose(f) != 0) return mdb::set_error(MDB_ERR_IO, "failed to write the checkpoint state");
+  return MDB_OK;
+}
+
+int mdb_sim_create_from_checkpoint(const mdb_config_t* cfg, const char* frame_path,
+                                   uint64_t frame_index, const char* state_path,
+                                   const mdb_options_t* opt, mdb_sim_t** out) {
+  if (!cfg || !frame_path || !state_path || !out)
+    return mdb::set_error(MDB_ERR_ARG, "null argument");
+  *out = nullptr;
+  FILE* f = fopen(state_path, "rb");
+  if (!f) return mdb::set_error(MDB_ERR_IO, std::string("cannot open ") + state_path);
+  std::string text;
+  char buf[4096];
+  size_t k;
+  while ((k = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, k);
+  fclose(f);
+  if (text.find(kCheckpointFormat) == std::string::npos)
+    return mdb::set_error(MDB_ERR_IO, "not a checkpoint state file");
+  Checkpoint c;
+  double v;
+  const struct {
+    const char* k;
+    double* p;
+  } dk[] = {{"t", &c.t},           {"Lx", &c.Lx},         {"Ly", &c.Ly},     {"xi", &c.xi},
+            {"K", &c.K},           {"pA", &c.pA},         {"aspect", &c.aspect},
+            {"P_cur", &c.P_cur},   {"last_P", &c.last_P}, {"fl", &c.fl},     {"ce", &c.ce},
+            {"vp", &c.vp},         {"Fp", &c.Fp},         {"wallU", &c.wallU},
+            {"p_ext", &c.p_ext}};
+  for (const auto& e : dk)
+    if (!ck_find(text, e.k, e.p))
+      return mdb::set_error(MDB_ERR_IO, std::string("checkpoint state lacks ") + e.k);
+  const struct {
+    const char* k;
+    int* p;
+  } ik[] = {{"clamped", &c.clamped},   {"piston_active", &c.piston_active},
+            {"nph_init", &c.nph_init}, {"vp_init", &c.vp_init},
+            {"k_valid", &c.k_valid},   {"p_valid", &c.p_valid},
+            {"periodic_y", &c.periodic_y}};
+  for (const auto& e : ik) {
+    if (!ck_find(text, e.k, &v))
+      return mdb::set_error(MDB_ERR_IO, std::string("checkpoint state lacks ") + e.k);
+    *e.p = (int)v;
+  }
+  if (!ck_find(text, "steps", &v)) return mdb::set_error(MDB_ERR_IO, "checkpoint state lacks steps");
+  c.steps = (int64_t)v;
+  // the box of the checkpoint, not the configuration's initial box
+  mdb_config_t cfg2 = *cfg;
+  cfg2.box_w_global = c.Lx;
+  cfg2.box_h_global = c.Ly;
+  mdb_sim_t* sim = nullptr;
+  MDB_TRY(mdb_sim_create_from_pframe(&cfg2, frame_path, frame_index, opt, &sim));
+  std::unique_ptr<mdb_sim> guard(sim);
+  if (c.periodic_y == 0) {
+    MDB_TRY(sim->eng->rebuild_now(0));
+    sim->periodic_y = 0;
+    MDB_TRY(sim->eng->force(mdb::FM_INIT, false));  // pair forces and walls
+  }
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  S.xi = c.xi;
+  S.K = c.K;
+  S.pA = c.pA;
+  S.aspect = c.aspect;
+  S.P_cur = c.P_cur;
+  S.last_P = c.last_P;
+  S.fl = c.fl;
+  S.ce = c.ce;
+  S.vp = c.vp;
+  S.Fp = c.Fp;
+  S.wallU = c.wallU;
+  S.p_ext = c.p_ext;
+  S.clamped = c.clamped;
+  S.steps = c.steps;
+  MDB_TRY(sim->eng->put_state(0, S));
+  sim->t = c.t;
+  sim->piston_active = c.piston_active != 0;
+  sim->nph_init = c.nph_init != 0;
+  sim->vp_init = c.vp_init != 0;
+  sim->k_valid = c.k_valid != 0;
+  sim->p_valid = c.p_valid != 0;
+  *out = guard.release();
+  return MDB_OK;
 }
 
 int mdb_sim_get_config(mdb_sim_t* sim, mdb_config_t* out) {

@@ -631,6 +631,19 @@ int Engine::get_frame(int s, mdb_particle_t* out) {
   return MDB_OK;
 }
 
+int Engine::export_async(int s, mdb_particle_t* host) {
+  MDB_CUDA(cudaSetDevice(device_));
+  const SysParams& P = hsp_[s];
+  const int g = (int)std::min<int64_t>((P.n + kThreads - 1) / kThreads, 4096);
+  k_export<<<g, kThreads, 0, stream_>>>(dev_, (DevParticle*)d_aos_, P.p0, P.n);
+  MDB_CUDA(cudaGetLastError());
+  launches_ += 1;
+  count_launches(1);
+  MDB_CUDA(cudaMemcpyAsync(host, d_aos_, sizeof(mdb_particle_t) * (size_t)P.n,
+                           cudaMemcpyDeviceToHost, stream_));
+  return MDB_OK;
+}
+
 int Engine::set_frame(int s, const mdb_particle_t* in) {
   MDB_CUDA(cudaSetDevice(device_));
   const SysParams& P = hsp_[s];

@@ -63,6 +63,10 @@ class Engine {
   int put_state(int s, const SysState& st);
   int get_frame(int s, mdb_particle_t* out);
   int set_frame(int s, const mdb_particle_t* in);
+  // Queues the export of system s's frame (caller's particle order) into
+  // `host` on the engine's stream and returns without waiting; `host` should
+  // be pinned memory for the copy to be asynchronous.
+  int export_async(int s, mdb_particle_t* host);
   // Slot -> original index and slot -> local cell of system s (n entries each).
   int debug_cells(int s, int32_t* orig, int32_t* cell);
   int sync();
@@ -112,5 +116,11 @@ class Engine {
 };
 
 int reference_initial_frame(const mdb_config_t& cfg, std::vector<mdb_particle_t>& out);
+
+// For the trajectory writer: queue the export of a simulation's frame into
+// `host` and record `ev` after it on the simulation's stream.
+int sim_export_async(mdb_sim_t* sim, mdb_particle_t* host, cudaEvent_t ev);
+int64_t sim_particles(mdb_sim_t* sim);
+int sim_device(mdb_sim_t* sim);
 
 }  // namespace mdb
