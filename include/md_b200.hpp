@@ -274,6 +274,23 @@ class MDSimulation {
 
   double cal_total_K() { return scalar(mdb_sim_total_K, "cal_total_K"); }
   double cal_total_U() { return scalar(mdb_sim_total_U, "cal_total_U"); }
+  // get_N_profile / get_density_profile / get_pressure_profile
+  // (src/md_env.cu:3821-4104), world size 1
+  std::vector<int> get_N_profile(int n_bins) {
+    std::vector<int> out((size_t)(n_bins > 0 ? 2 * n_bins : 0));
+    check(mdb_sim_n_profile(sim_, n_bins, out.data()), "get_N_profile");
+    return out;
+  }
+  std::vector<double> get_density_profile(int n_bins) {
+    std::vector<double> out((size_t)(n_bins > 0 ? n_bins : 0));
+    check(mdb_sim_density_profile(sim_, n_bins, out.data()), "get_density_profile");
+    return out;
+  }
+  std::vector<double> get_pressure_profile(int n_bins) {
+    std::vector<double> out((size_t)(n_bins > 0 ? 3 * n_bins : 0));
+    check(mdb_sim_pressure_profile(sim_, n_bins, out.data()), "get_pressure_profile");
+    return out;
+  }
   // cal_partial_U_lambda (src/md_env.cu:2362-2406)
   double cal_partial_U_lambda(double epsilon_lambda) {
     double v = 0.0;

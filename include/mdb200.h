@@ -188,6 +188,22 @@ int mdb_sim_total_U(mdb_sim_t* sim, double* out);
  * sums), y periodic unless the piston mode is active. The reference counts
  * x-edge partners twice at MPI world size 1; this is the nearest-image sum. */
 int mdb_sim_partial_U_lambda(mdb_sim_t* sim, double epsilon_lambda, double* out);
+/* get_N_profile (src/md_env.cu:3920-3985, kernel src/md_cuda_common.cu:827-871)
+ * at MPI world size 1: counts of type 0 in out[0..nb) and of the other types
+ * in out[nb..2nb), in nb equal x bins over [0, Lx]. */
+int mdb_sim_n_profile(mdb_sim_t* sim, int32_t nb, int32_t* out);
+/* get_density_profile (src/md_env.cu:4086-4104): (n_A - n_B) / (n_A + n_B)
+ * per x bin, 0 for an empty bin; out holds nb doubles. */
+int mdb_sim_density_profile(mdb_sim_t* sim, int32_t nb, double* out);
+/* get_pressure_profile (src/md_env.cu:3821-3918, kernel
+ * src/md_cuda_common.cu:873-1030): Irving-Kirkwood pressure tensor in nb y
+ * bins, out[3*nb] = {P_xx | P_yy | P_xy}: kinetic m v_a v_b at the bin of
+ * y_i, pair 1/2 r_a F_b at the bin of the minimum-image midpoint, divided by
+ * the bin area Lx * Ly / nb. Pairs from the cell stencil; sums in 64-bit
+ * fixed point (2^-24), so the result does not depend on thread order. The y
+ * axis is periodic unless the piston mode is active (the reference always
+ * treats it as periodic). */
+int mdb_sim_pressure_profile(mdb_sim_t* sim, int32_t nb, double* out);
 /* cal_instant_pressure (src/md_env.cu:2254-2266). */
 int mdb_sim_instant_pressure(mdb_sim_t* sim, double* out);
 

@@ -9,6 +9,8 @@ Python mirror of the reference's C++ surface for the hot path, over the C ABI of
                                       — include/md_energy_minimizer.hpp:11-97
 * ``FileWriter`` / ``FileReader``     — include/md_common.hpp:88-122 (PFRAME v2)
 * ``Batch``                           — many independent systems in one launch
+* ``Server``                          — continuous batching of MD / FIRE requests
+* ``TrajectoryWriter``                — asynchronous PFRAME writer
 
 Frames are numpy arrays of ``PARTICLE_DTYPE`` (the 64-byte Particle of
 include/md_particle.hpp:31-38). The MPI communicator arguments of the reference
@@ -34,8 +36,10 @@ REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 __all__ = [
     "PARTICLE_DTYPE", "MDBError", "MDConfig", "MDConfigManager", "MDSimulation",
-    "EnergyMinimizer", "FireParams", "MinimizeResult", "FileWriter", "FileReader", "Batch",
-    "make_frame", "compute_forces", "cell_build", "kernel_launches",
+    "EnergyMinimizer", "FireParams", "MinimizeResult", "FileWriter", "FileReader",
+    "TrajectoryWriter", "Batch", "Server", "RequestResult", "make_frame", "compute_forces",
+    "cell_build", "kernel_launches", "JOB_FIRE", "JOB_NVE", "JOB_NVT", "REQ_QUEUED",
+    "REQ_RUNNING", "REQ_DONE", "REQ_FAILED",
 ]
 
 MDConfig = MDBConfigC  # field-for-field MDConfig
@@ -214,6 +218,27 @@ class MDSimulation:
         v = C.c_double()
         check(lib().mdb_sim_partial_U_lambda(self._h, float(epsilon_lambda), C.byref(v)))
         return v.value
+
+    def get_N_profile(self, n_bins: int) -> np.ndarray:
+        """get_N_profile: [count of type 0 per x bin..., count of others...]."""
+        out = np.zeros(2 * n_bins, dtype=np.int32)
+        check(lib().mdb_sim_n_profile(self._h, int(n_bins),
+                                      out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
+
+    def get_density_profile(self, n_bins: int) -> np.ndarray:
+        """get_density_profile: (n_A - n_B) / (n_A + n_B) per x bin."""
+        out = np.zeros(n_bins)
+        check(lib().mdb_sim_density_profile(self._h, int(n_bins),
+                                            out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def get_pressure_profile(self, n_bins: int) -> np.ndarray:
+        """get_pressure_profile: [Pxx..., Pyy..., Pxy...] per y bin."""
+        out = np.zeros(3 * n_bins)
+        check(lib().mdb_sim_pressure_profile(self._h, int(n_bins),
+                                             out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
 
     def cal_instant_pressure(self) -> float:
         return self._scalar(lib().mdb_sim_instant_pressure)

@@ -230,6 +230,9 @@ SIGNATURES = {
     "mdb_sim_total_U": ([_vp, _dp], C.c_int),
     "mdb_sim_instant_pressure": ([_vp, _dp], C.c_int),
     "mdb_sim_partial_U_lambda": ([_vp, C.c_double, _dp], C.c_int),
+    "mdb_sim_n_profile": ([_vp, C.c_int32, _ip], C.c_int),
+    "mdb_sim_density_profile": ([_vp, C.c_int32, _dp], C.c_int),
+    "mdb_sim_pressure_profile": ([_vp, C.c_int32, _dp], C.c_int),
     "mdb_sim_observables": ([_vp, C.POINTER(MDBObservables)], C.c_int),
     "mdb_sim_get_frame": ([_vp, _vp, C.c_int64], C.c_int),
     "mdb_sim_set_frame": ([_vp, _vp, C.c_int64], C.c_int),

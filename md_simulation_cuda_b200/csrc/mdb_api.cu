@@ -258,6 +258,36 @@ int mdb_sim_partial_U_lambda(mdb_sim_t* sim, double epsilon_lambda, double* out)
   return check_status(sim);
 }
 
+int mdb_sim_n_profile(mdb_sim_t* sim, int32_t nb, int32_t* out) {
+  if (!sim || !out || nb <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  return sim->eng->profiles(0, nb, sim->periodic_y != 0, nullptr, out);
+}
+
+int mdb_sim_density_profile(mdb_sim_t* sim, int32_t nb, double* out) {
+  if (!sim || !out || nb <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  std::vector<int32_t> c((size_t)2 * nb);
+  MDB_TRY(sim->eng->profiles(0, nb, sim->periodic_y != 0, nullptr, c.data()));
+  // get_density_profile (src/md_env.cu:4086-4104)
+  for (int32_t k = 0; k < nb; ++k) {
+    const double a = (double)c[k], b = (double)c[nb + k];
+    const double sum = a + b;
+    out[k] = (sum == 0.0) ? 0.0 : (a - b) / sum;
+  }
+  return MDB_OK;
+}
+
+int mdb_sim_pressure_profile(mdb_sim_t* sim, int32_t nb, double* out) {
+  if (!sim || !out || nb <= 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  std::vector<double> acc((size_t)3 * nb);
+  MDB_TRY(sim->eng->profiles(0, nb, sim->periodic_y != 0, acc.data(), nullptr));
+  SysState S;
+  MDB_TRY(sim->eng->get_state(0, &S));
+  // per bin area Lx * (Ly / nb) (src/md_env.cu:3899-3916)
+  const double vol = S.Lx * (S.Ly / (double)nb);
+  for (size_t k = 0; k < acc.size(); ++k) out[k] = (vol > 0.0) ? acc[k] / vol : acc[k];
+  return check_status(sim);
+}
+
 int mdb_sim_instant_pressure(mdb_sim_t* sim, double* out) {
   if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
   MDB_TRY(sim->eng->force(mdb::FM_OBS, !sim->piston_active));

@@ -631,6 +631,44 @@ int Engine::get_frame(int s, mdb_particle_t* out) {
   return MDB_OK;
 }
 
+int Engine::profiles(int s, int nb, bool py, double* ptens, int32_t* counts) {
+  MDB_CUDA(cudaSetDevice(device_));
+  unsigned long long* d_acc = nullptr;
+  int* d_cnt = nullptr;
+  MDB_CUDA(cudaMalloc(&d_acc, sizeof(unsigned long long) * 3 * (size_t)nb));
+  cudaError_t e = cudaMalloc(&d_cnt, sizeof(int) * 2 * (size_t)nb);
+  if (e != cudaSuccess) {
+    cudaFree(d_acc);
+    return cuda_error(e, "cudaMalloc (profiles)");
+  }
+  e = cudaMemsetAsync(d_acc, 0, sizeof(unsigned long long) * 3 * (size_t)nb, stream_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt, 0, sizeof(int) * 2 * (size_t)nb, stream_);
+  if (e == cudaSuccess) {
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>((hsp_[s].n + kThreads - 1) / kThreads, 4096));
+    if (py)
+      k_profiles<true><<<g, kThreads, 0, stream_>>>(dev_, s, nb, d_acc, d_cnt);
+    else
+      k_profiles<false><<<g, kThreads, 0, stream_>>>(dev_, s, nb, d_acc, d_cnt);
+    e = cudaGetLastError();
+    launches_ += 1;
+    count_launches(1);
+  }
+  std::vector<long long> acc((size_t)3 * nb);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(acc.data(), d_acc, sizeof(long long) * acc.size(), cudaMemcpyDeviceToHost,
+                        stream_);
+  if (e == cudaSuccess && counts)
+    e = cudaMemcpyAsync(counts, d_cnt, sizeof(int) * 2 * (size_t)nb, cudaMemcpyDeviceToHost,
+                        stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(d_acc);
+  cudaFree(d_cnt);
+  if (e != cudaSuccess) return cuda_error(e, "profiles");
+  if (ptens)
+    for (size_t k = 0; k < acc.size(); ++k) ptens[k] = (double)acc[k] / kProfileFix;
+  return MDB_OK;
+}
+
 int Engine::export_async(int s, mdb_particle_t* host) {
   MDB_CUDA(cudaSetDevice(device_));
   const SysParams& P = hsp_[s];

@@ -67,6 +67,10 @@ class Engine {
   // `host` on the engine's stream and returns without waiting; `host` should
   // be pinned memory for the copy to be asynchronous.
   int export_async(int s, mdb_particle_t* host);
+  // Per-type x-bin counts (2*nb ints) and unnormalised Irving-Kirkwood sums
+  // in y bins (3*nb doubles: xx | yy | xy) of system s; py selects the y
+  // convention of the engine's current cell binning.
+  int profiles(int s, int nb, bool py, double* ptens, int32_t* counts);
   // Slot -> original index and slot -> local cell of system s (n entries each).
   int debug_cells(int s, int32_t* orig, int32_t* cell);
   int sync();

@@ -375,6 +375,19 @@ __device__ __forceinline__ void split_box(double L, float& h, float& l, float& i
   inv = 1.0f / h;
 }
 
+// Pair parameters of slot i's class: "same" for partners of its own class,
+// "ab" otherwise (types other than 0/1 always use AB).
+__device__ __forceinline__ void set_profile_class(PairCtx& c, const SysParams& P, int tci) {
+  c.ts = (tci == 2) ? 99u : (uint32_t)tci;
+  const int sc = (tci == 2) ? 2 : tci;
+  c.rc2s = P.frc2[sc];
+  c.rc2ab = P.frc2[2];
+  c.sig2s = P.fsig2[sc];
+  c.sig2ab = P.fsig2[2];
+  c.e24s = P.feps24[sc];
+  c.e24ab = P.feps24[2];
+}
+
 // Sum of pair forces on slot i over its 3x3 cell stencil (or every slot of the
 // system for grids narrower than 3 cells). Returns F in FP64.
 template <bool PY, bool ENERGY, bool VIRIAL>
@@ -1297,6 +1310,127 @@ __global__ void k_rb_finish(Dev D) {
   }
   __syncthreads();
   if (threadIdx.x == 0) D.bg->any_rebuild = 0;
+}
+
+// ------------------------------------------------------------ profiles --
+// get_N_profile / get_pressure_profile (src/md_cuda_common.cu:827-1030) for
+// system s: per-type counts in x bins, and the Irving-Kirkwood pressure
+// tensor in y bins (kinetic m v_a v_b at the bin of y_i, pair 1/2 r_a F_b at
+// the bin of the minimum-image midpoint y_i - dy/2). Pairs come from the cell
+// stencil of the last rebuild (exact while the rebuild criterion holds).
+// Sums are fixed point (2^-24) in 64-bit integers, so atomics give the same
+// result in any order.
+constexpr double kProfileFix = 16777216.0;
+
+__device__ __forceinline__ int profile_bin(double y, double Ly, int nb, bool py) {
+  double yy = py ? pbc_wrap(y, Ly) : y;
+  if (!py) {
+    if (yy < 0.0)
+      yy = 0.0;
+    else if (yy >= Ly && Ly > 0.0)
+      yy = Ly * (1.0 - 1e-12);
+  }
+  const double t = (Ly > 0.0) ? (yy / Ly) : 0.0;
+  int b = (int)(t * (double)nb);
+  return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+}
+
+__device__ __forceinline__ void fix_add(unsigned long long* a, double v) {
+  atomicAdd(a, (unsigned long long)__double2ll_rn(v * kProfileFix));
+}
+
+template <bool PY>
+__global__ void __launch_bounds__(kThreads) k_profiles(Dev D, int s, int nb,
+                                                       unsigned long long* ptens, int* counts) {
+  const SysParams& P = D.sp[s];
+  const SysState& S = D.st[s];
+  const double Lx = S.Lx, Ly = S.Ly;
+  PairCtx c;
+  split_box(Lx, c.Lxh, c.Lxl, c.invLx);
+  split_box(Ly, c.Lyh, c.Lyl, c.invLy);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P.n; k += stride) {
+    const int64_t i = P.p0 + k;
+    const double2 p = D.pos[i];
+    const double2 v = D.vel[i];
+    const int ti = D.type[i];
+    if (p.x >= 0.0 && p.x <= Lx) {
+      int b = (int)(p.x / Lx * nb);
+      b = b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+      atomicAdd(counts + (ti == 0 ? 0 : nb) + b, 1);
+    }
+    const double m = type_mass(P, ti);
+    const int bk = profile_bin(p.y, Ly, nb, PY);
+    fix_add(ptens + bk, m * v.x * v.x);
+    fix_add(ptens + nb + bk, m * v.y * v.y);
+    fix_add(ptens + 2 * nb + bk, m * v.x * v.y);
+    const float4 qi = D.pff[i];
+    c.xih = fabsf(qi.x);
+    c.yih = fabsf(qi.y);
+    c.xil = qi.z;
+    c.yil = qi.w;
+    set_profile_class(c, P, type_class(ti));
+    // candidate ranges: the whole system, or the 3x3 stencil
+    int r0[6], r1[6], nr = 0;
+    if (S.allpairs) {
+      r0[0] = (int)P.p0;
+      r1[0] = (int)(P.p0 + P.n);
+      nr = 1;
+    } else {
+      const int ncx = S.ncx, ncy = S.ncy;
+      const int cell = D.cell_of[i];
+      const int cx = cell % ncx, cy = cell / ncx;
+      for (int dr = -1; dr <= 1; ++dr) {
+        int yy = cy + dr;
+        if (PY) {
+          if (yy < 0) yy += ncy;
+          if (yy >= ncy) yy -= ncy;
+        } else if (yy < 0 || yy >= ncy) {
+          continue;
+        }
+        const int64_t row = P.c0 + (int64_t)yy * ncx;
+        if (cx > 0 && cx < ncx - 1) {
+          r0[nr] = D.cstart[row + cx - 1];
+          r1[nr++] = D.cstart[row + cx + 2];
+        } else if (cx == 0) {
+          r0[nr] = D.cstart[row];
+          r1[nr++] = D.cstart[row + 2];
+          r0[nr] = D.cstart[row + ncx - 1];
+          r1[nr++] = D.cstart[row + ncx];
+        } else {
+          r0[nr] = D.cstart[row + ncx - 2];
+          r1[nr++] = D.cstart[row + ncx];
+          r0[nr] = D.cstart[row];
+          r1[nr++] = D.cstart[row + 1];
+        }
+      }
+    }
+    for (int r = 0; r < nr; ++r) {
+      for (int j = r0[r]; j < r1[r]; ++j) {
+        if (j == i) continue;
+        const float4 q = D.pff[j];
+        float dx, dy;
+        const float r2 = pair_r2<PY>(q, c, dx, dy);
+        const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
+        const bool same = (tj == c.ts);
+        const float rc2 = same ? c.rc2s : c.rc2ab;
+        if (!(r2 > 0.0f && r2 < rc2)) continue;
+        const float sig2 = same ? c.sig2s : c.sig2ab;
+        const float e24 = same ? c.e24s : c.e24ab;
+        const float r2i = 1.0f / r2;
+        const float sr2 = sig2 * r2i;
+        const float sr6 = sr2 * sr2 * sr2;
+        const float sr12 = sr6 * sr6;
+        const float tmp = e24 * fmaf(2.0f, sr12, -sr6) * r2i;
+        const double ddx = (double)dx, ddy = (double)dy;
+        const double Fx = (double)(tmp * dx), Fy = (double)(tmp * dy);
+        const int bp = profile_bin(p.y - 0.5 * ddy, Ly, nb, PY);
+        fix_add(ptens + bp, 0.5 * ddx * Fx);
+        fix_add(ptens + nb + bp, 0.5 * ddy * Fy);
+        fix_add(ptens + 2 * nb + bp, 0.5 * ddx * Fy);
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------ frame I/O --

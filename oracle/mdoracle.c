@@ -496,6 +496,109 @@ int or_partial_U_lambda(const or_lj_t* lj, int64_t n, const double* pos, const i
   return 0;
 }
 
+/* get_N_profile (src/md_env.cu:3920-3985, kernel src/md_cuda_common.cu:827-871)
+ * at world size 1 (x_min = 0, x_max = Lx): counts of type 0 in out[0..nb) and
+ * of other types in out[nb..2nb), bin = int(x / Lx * nb) clamped, particles
+ * with 0 <= x <= Lx. */
+int or_n_profile(int64_t n, const double* pos, const int32_t* type, double Lx, int32_t nb,
+                 int32_t* out) {
+  if (nb <= 0 || !out) return 1;
+  memset(out, 0, sizeof(int32_t) * 2 * (size_t)nb);
+  for (int64_t i = 0; i < n; ++i) {
+    const double x = pos[2 * i];
+    if (!(x >= 0.0 && x <= Lx)) continue;
+    int b = (int)(x / Lx * nb);
+    if (b < 0) b = 0;
+    if (b >= nb) b = nb - 1;
+    out[(type[i] == 0 ? 0 : nb) + b] += 1;
+  }
+  return 0;
+}
+
+static int profile_bin(double y, double Ly, int32_t nb, int periodic_y) {
+  double yy = periodic_y ? or_pbc_wrap(y, Ly) : y;
+  if (!periodic_y) {
+    if (yy < 0.0)
+      yy = 0.0;
+    else if (yy >= Ly && Ly > 0.0)
+      yy = Ly * (1.0 - 1e-12);
+  }
+  const double t = (Ly > 0.0) ? (yy / Ly) : 0.0;
+  int b = (int)(t * (double)nb);
+  if (b < 0) b = 0;
+  if (b >= nb) b = nb - 1;
+  return b;
+}
+
+/* get_pressure_profile (src/md_env.cu:3821-3918, kernel
+ * src/md_cuda_common.cu:873-1030), all pairs with the nearest image:
+ * out[0..nb) = P_xx, [nb..2nb) = P_yy, [2nb..3nb) = P_xy per y bin; kinetic
+ * m v_a v_b at the bin of y_i, pair 1/2 r_a F_b at the bin of the midpoint
+ * y_i - dy/2, each divided by the bin area Lx * Ly / nb. FP64 or the
+ * reference's mixed arithmetic. */
+int or_pressure_profile(const or_lj_t* lj, int64_t n, const double* pos, const double* vel,
+                        const int32_t* type, double Lx, double Ly, int32_t periodic_y,
+                        int32_t mode, int32_t nb, double* out) {
+  if (nb <= 0 || !out) return 1;
+  memset(out, 0, sizeof(double) * 3 * (size_t)nb);
+  const float Lx_f = (float)Lx, Ly_f = (float)Ly;
+  for (int64_t i = 0; i < n; ++i) {
+    const double m = type_mass(lj, type[i]);
+    const double vx = vel[2 * i], vy = vel[2 * i + 1];
+    const int bk = profile_bin(pos[2 * i + 1], Ly, nb, periodic_y);
+    out[bk] += m * vx * vx;
+    out[nb + bk] += m * vy * vy;
+    out[2 * nb + bk] += m * vx * vy;
+    for (int64_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const int c = pair_class(type[i], type[j]);
+      double dx, dy, Fx, Fy;
+      if (mode == OR_FP64) {
+        dx = pos[2 * i] - pos[2 * j];
+        dy = pos[2 * i + 1] - pos[2 * j + 1];
+        dx = dx - Lx * round(dx / Lx);
+        if (periodic_y) dy = dy - Ly * round(dy / Ly);
+        const double sig = lj->sigma[c], rc = lj->cutoff * sig;
+        const double r2 = dx * dx + dy * dy;
+        if (!(r2 > 0.0 && r2 < rc * rc)) continue;
+        const double r2i = 1.0 / r2;
+        const double sr2 = sig * sig * r2i;
+        const double sr6 = sr2 * sr2 * sr2;
+        const double sr12 = sr6 * sr6;
+        const double tmp = 24.0 * lj->epsilon[c] * (2.0 * sr12 - sr6) * r2i;
+        Fx = tmp * dx;
+        Fy = tmp * dy;
+      } else {
+        float dx_f = (float)(pos[2 * i] - pos[2 * j]);
+        float dy_f = (float)(pos[2 * i + 1] - pos[2 * j + 1]);
+        dx_f = fmaf(-Lx_f, roundf(dx_f / Lx_f), dx_f);
+        if (periodic_y) dy_f = fmaf(-Ly_f, roundf(dy_f / Ly_f), dy_f);
+        const float sigma_f = (float)lj->sigma[c];
+        const float rc_f = (float)lj->cutoff * sigma_f;
+        const float dr_sq_f = fmaf(dx_f, dx_f, dy_f * dy_f);
+        if (!(dr_sq_f > 0.0f && dr_sq_f < rc_f * rc_f)) continue;
+        const float r2_inv_f = 1.0f / dr_sq_f;
+        const float sr2_f = (sigma_f * sigma_f) * r2_inv_f;
+        const float sr6_f = sr2_f * sr2_f * sr2_f;
+        const float sr12_f = sr6_f * sr6_f;
+        const float tmp_f = (24.0f * (float)lj->epsilon[c]) * fmaf(2.0f, sr12_f, -sr6_f) * r2_inv_f;
+        dx = (double)dx_f;
+        dy = (double)dy_f;
+        Fx = (double)(tmp_f * dx_f);
+        Fy = (double)(tmp_f * dy_f);
+      }
+      const int bp = profile_bin(pos[2 * i + 1] - 0.5 * dy, Ly, nb, periodic_y);
+      out[bp] += 0.5 * dx * Fx;
+      out[nb + bp] += 0.5 * dy * Fy;
+      out[2 * nb + bp] += 0.5 * dx * Fy;
+    }
+  }
+  const double vol = Lx * (Ly / (double)nb);
+  if (vol > 0.0)
+    for (int k = 0; k < 3 * nb; ++k) out[k] /= vol;
+  return 0;
+}
+
 /* ---- engine --------------------------------------------------------------- */
 static void sim_forces(or_sim_t* s, int32_t periodic_y, double* acc, double* U, double* W) {
   if (s->use_cells && !s->ws1_halo)

@@ -74,6 +74,15 @@ int or_forces_rows(const or_lj_t* lj, int64_t n, const double* pos, const int32_
 int or_partial_U_lambda(const or_lj_t* lj, int64_t n, const double* pos, const int32_t* type,
                         double Lx, double Ly, int32_t periodic_y, int32_t mode,
                         double epsilon_lambda, double* out, double* scale, int32_t nthreads);
+/* get_N_profile at world size 1 (src/md_env.cu:3920-3985): per-type counts
+ * in x bins, out[2*nb] = {type 0 | other types}. */
+int or_n_profile(int64_t n, const double* pos, const int32_t* type, double Lx, int32_t nb,
+                 int32_t* out);
+/* get_pressure_profile (src/md_env.cu:3821-3918): Irving-Kirkwood profile
+ * in y bins, out[3*nb] = {Pxx | Pyy | Pxy}, all pairs, nearest image. */
+int or_pressure_profile(const or_lj_t* lj, int64_t n, const double* pos, const double* vel,
+                        const int32_t* type, double Lx, double Ly, int32_t periodic_y,
+                        int32_t mode, int32_t nb, double* out);
 /* Ordered in-cutoff pairs counted through a cell list (large systems). */
 int64_t or_count_pairs_cells(const or_lj_t* lj, int64_t n, const double* pos,
                              const int32_t* type, double Lx, double Ly, int32_t nthreads);

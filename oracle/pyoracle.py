@@ -117,6 +117,9 @@ def lib():
             L.or_count_pairs.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
                                          C.c_double, C.c_int32, C.c_int32]
             L.or_count_pairs.restype = C.c_int64
+            L.or_n_profile.argtypes = [C.c_int64, dp, ip, C.c_double, C.c_int32, ip]
+            L.or_pressure_profile.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, dp, ip, C.c_double,
+                                              C.c_double, C.c_int32, C.c_int32, C.c_int32, dp]
             L.or_partial_U_lambda.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
                                               C.c_double, C.c_int32, C.c_int32, C.c_double, dp,
                                               dp, C.c_int32]
@@ -217,6 +220,27 @@ def partial_U_lambda(cfg, pos, types, Lx, Ly, eps_lambda, periodic_y=1, mode=0, 
                                    nthreads)
     assert rc == 0
     return out.value, scale.value
+
+
+def n_profile(pos, types, Lx, nb):
+    """get_N_profile: (counts of type 0, counts of other types) in x bins."""
+    p = _pos2(pos)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    out = np.zeros(2 * nb, dtype=np.int32)
+    assert lib().or_n_profile(p.shape[0], _dp(p), _ip(t), Lx, nb, _ip(out)) == 0
+    return out[:nb], out[nb:]
+
+
+def pressure_profile(cfg, pos, vel, types, Lx, Ly, nb, periodic_y=1, mode=0):
+    """get_pressure_profile: (Pxx, Pyy, Pxy) in y bins."""
+    p = _pos2(pos)
+    v = _pos2(vel)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    lj = make_lj(cfg)
+    out = np.zeros(3 * nb)
+    assert lib().or_pressure_profile(C.byref(lj), p.shape[0], _dp(p), _dp(v), _ip(t), Lx, Ly,
+                                     periodic_y, mode, nb, _dp(out)) == 0
+    return out[:nb], out[nb:2 * nb], out[2 * nb:]
 
 
 def count_pairs_cells(cfg, pos, types, Lx, Ly, nthreads=0):

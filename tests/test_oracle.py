@@ -164,3 +164,22 @@ def test_partial_U_lambda_two_particles():
             tol = 1e-12 if mode == po.OR_FP64 else 1e-4
             assert abs(vx + 0.01 * tmp * r * r) <= tol * abs(tmp * r * r) * 0.01 + 1e-14
             assert abs(vy - 0.01 * tmp * r * r) <= tol * abs(tmp * r * r) * 0.01 + 1e-14
+
+
+def test_pressure_profile_sum_rule():
+    """Summed over the bins, the Irving-Kirkwood profile gives back the scalar
+    pressure's parts: sum (Pxx + Pyy) * bin area = sum m v^2 + W, with
+    W = 1/2 sum over ordered pairs of r.F (src/md_cuda_common.cu:873-1030 vs
+    :591-701)."""
+    from md_simulation_cuda_b200 import workloads as wl
+
+    f, Lx, Ly = wl.lattice_frame(400, 0.8, 1.0, 0.65, 1.0, seed=1)
+    cfg = wl.config_dict(400, Lx, Ly, dt=0.001)
+    nb = 10
+    xx, yy, xy = po.pressure_profile(cfg, f["pos"], f["vel"], f["type"], Lx, Ly, nb)
+    kin = float((f["vel"] ** 2).sum())  # unit masses
+    _, _, W = po.forces(cfg, f["pos"], f["type"], Lx, Ly, mode=po.OR_FP64)
+    total = (xx.sum() + yy.sum()) * (Lx * Ly / nb)
+    assert abs(total - (kin + W)) <= 1e-9 * (kin + abs(W))
+    a, b = po.n_profile(f["pos"], f["type"], Lx, nb)
+    assert a.sum() + b.sum() == 400 and a.sum() == int((f["type"] == 0).sum())
