@@ -275,6 +275,64 @@ int mdb_traj_writer_write(mdb_traj_writer_t* w, mdb_sim_t* sim, uint64_t frame_i
 int mdb_traj_writer_flush(mdb_traj_writer_t* w);
 int mdb_traj_writer_close(mdb_traj_writer_t* w);
 
+/* ---- NPH driver protocol ---------------------------------------------------
+ * The protocol of the reference's NPH driver (tests/run_NPH_test/
+ * run_test_NPH.cpp:137-290): AUTO_TARGET (Nose-Hoover steps; the pressure
+ * sampled every eval_interval steps, averaged over auto_steps steps, becomes
+ * the target) -> NPH_WARMUP (NPH steps at the target; once warmup_min_steps
+ * have run and the rolling window of window_samples samples is full, each
+ * step whose window mean and standard deviation are within tolerance_rel of
+ * the target counts, stable_required such steps in a row end the warmup; it
+ * ends anyway after warmup_max_steps) -> NPH_PRODUCTION (production_steps NPH
+ * steps). Steps between two points where the protocol samples or decides run
+ * as captured chunks; the decisions fall on the same steps as in the per-step
+ * loop. records (up to cap) receive one entry per sample step, like the
+ * driver's pressure log. */
+typedef struct mdb_nph_protocol {
+  int32_t auto_target;   /* 1: start with AUTO_TARGET ("auto_initial" mode)  */
+  int32_t _pad0;
+  double P_target;       /* the target when auto_target == 0                  */
+  int32_t auto_steps, eval_interval, window_samples, stable_required;
+  int32_t warmup_min_steps, warmup_max_steps, production_steps, _pad1;
+  double tolerance_rel;
+  int32_t reserved[8];
+} mdb_nph_protocol_t;
+
+#define MDB_PHASE_AUTO_TARGET 0
+#define MDB_PHASE_NPH_WARMUP 1
+#define MDB_PHASE_NPH_PRODUCTION 2
+
+typedef struct mdb_nph_record {
+  int64_t step;
+  double t;
+  int32_t phase; /* MDB_PHASE_* the step ran in */
+  int32_t _pad;
+  double P_inst, P_target, mean, stddev, rel_err; /* rolling window stats */
+  double Lx, Ly, dA_dt;
+} mdb_nph_record_t;
+
+typedef struct mdb_nph_result {
+  double P_target;
+  int64_t auto_end_step;   /* -1 when there was no AUTO_TARGET phase        */
+  int64_t warmup_end_step; /* -1 when the warmup did not end                */
+  int64_t total_steps;
+  int64_t n_records;       /* sample steps (may exceed cap)                 */
+  int32_t forced_switch;   /* the warmup ended at warmup_max_steps          */
+  int32_t finished;        /* production completed                          */
+} mdb_nph_result_t;
+
+/* The protocol parameters as the driver derives them from MDConfig
+ * (pressure_target_mode, P_target, pressure_*, nph_warmup_*, nph_steps). */
+int mdb_nph_protocol_from_config(const mdb_config_t* cfg, mdb_nph_protocol_t* out);
+int mdb_sim_run_nph_protocol(mdb_sim_t* sim, const mdb_nph_protocol_t* protocol,
+                             mdb_nph_record_t* records, int64_t cap, mdb_nph_result_t* result);
+/* The protocol's decisions for a given pressure per step (pressures[step],
+ * n entries), without a simulation; chunks receives the number of step
+ * chunks the real run would issue. */
+int mdb_nph_protocol_dry_run(const mdb_nph_protocol_t* protocol, const double* pressures,
+                             int64_t n, mdb_nph_record_t* records, int64_t cap,
+                             mdb_nph_result_t* result, int64_t* chunks);
+
 /* ---- FIRE minimiser (class EnergyMinimizer, include/md_energy_minimizer.hpp)
  */
 typedef struct mdb_fire_params { /* FireParams (md_energy_minimizer.hpp:11-25) */

@@ -27,8 +27,9 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from ._lib import (MDB_ERR_ARG, MDBConfigC, MDBError, MDBFireParams, MDBMinimizeResult,
-                   MDBObservables, MDBRequest, MDBRequestResult, MDBServerOptions,
-                   MDBServerStats, PARTICLE_DTYPE, check, frame_ptr, lib, options)
+                   MDBNphProtocol, MDBNphRecord, MDBNphResult, MDBObservables, MDBRequest,
+                   MDBRequestResult, MDBServerOptions, MDBServerStats, PARTICLE_DTYPE, check,
+                   frame_ptr, lib, options)
 
 # job kinds (mdb200.h MDB_JOB_*) and request states (MDB_REQ_*)
 JOB_FIRE, JOB_NVE, JOB_NVT = 0, 1, 2
@@ -240,6 +241,19 @@ class MDSimulation:
                                              out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
+    def run_nph_protocol(self, protocol: Optional[MDBNphProtocol] = None,
+                         record_cap: int = 100000):
+        """The NPH driver protocol (AUTO_TARGET -> NPH_WARMUP -> NPH_PRODUCTION of
+        tests/run_NPH_test/run_test_NPH.cpp); parameters from the config unless
+        given. Returns (result, records)."""
+        if protocol is None:
+            protocol = nph_protocol_from_config(self.cfg_manager)
+        recs = (MDBNphRecord * max(1, record_cap))()
+        res = MDBNphResult()
+        check(lib().mdb_sim_run_nph_protocol(self._h, C.byref(protocol), recs, record_cap,
+                                             C.byref(res)))
+        return res, list(recs[:min(res.n_records, record_cap)])
+
     def cal_instant_pressure(self) -> float:
         return self._scalar(lib().mdb_sim_instant_pressure)
 
@@ -411,6 +425,26 @@ class FileWriter:
         check(lib().mdb_pframe_write(os.fsencode(self.path), 0 if self._fresh else 1,
                                      frame_ptr(f), len(f), int(frame_index)))
         self._fresh = False
+
+
+def nph_protocol_from_config(config) -> MDBNphProtocol:
+    """NPH protocol parameters as the reference's driver derives them."""
+    p = MDBNphProtocol()
+    check(lib().mdb_nph_protocol_from_config(C.byref(_config_of(config)), C.byref(p)))
+    return p
+
+
+def nph_protocol_dry_run(protocol: MDBNphProtocol, pressures, record_cap: int = 100000):
+    """The protocol's decisions for given pressures per step (no GPU):
+    (result, records, chunks)."""
+    p = np.ascontiguousarray(pressures, dtype=np.float64)
+    recs = (MDBNphRecord * max(1, record_cap))()
+    res = MDBNphResult()
+    chunks = C.c_int64()
+    check(lib().mdb_nph_protocol_dry_run(C.byref(protocol),
+                                         p.ctypes.data_as(C.POINTER(C.c_double)), len(p),
+                                         recs, record_cap, C.byref(res), C.byref(chunks)))
+    return res, list(recs[:min(res.n_records, record_cap)]), chunks.value
 
 
 class TrajectoryWriter:

@@ -199,6 +199,34 @@ class MDBServerStats(C.Structure):
     ]
 
 
+class MDBNphProtocol(C.Structure):
+    _fields_ = [
+        ("auto_target", C.c_int32), ("_pad0", C.c_int32), ("P_target", C.c_double),
+        ("auto_steps", C.c_int32), ("eval_interval", C.c_int32),
+        ("window_samples", C.c_int32), ("stable_required", C.c_int32),
+        ("warmup_min_steps", C.c_int32), ("warmup_max_steps", C.c_int32),
+        ("production_steps", C.c_int32), ("_pad1", C.c_int32),
+        ("tolerance_rel", C.c_double), ("reserved", C.c_int32 * 8),
+    ]
+
+
+class MDBNphRecord(C.Structure):
+    _fields_ = [
+        ("step", C.c_int64), ("t", C.c_double), ("phase", C.c_int32), ("_pad", C.c_int32),
+        ("P_inst", C.c_double), ("P_target", C.c_double), ("mean", C.c_double),
+        ("stddev", C.c_double), ("rel_err", C.c_double), ("Lx", C.c_double),
+        ("Ly", C.c_double), ("dA_dt", C.c_double),
+    ]
+
+
+class MDBNphResult(C.Structure):
+    _fields_ = [
+        ("P_target", C.c_double), ("auto_end_step", C.c_int64),
+        ("warmup_end_step", C.c_int64), ("total_steps", C.c_int64),
+        ("n_records", C.c_int64), ("forced_switch", C.c_int32), ("finished", C.c_int32),
+    ]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -285,6 +313,12 @@ SIGNATURES = {
                         _ip, _ip], C.c_int),
     "mdb_compute_forces_noalloc": ([_cfgp, _vp, _vp, C.c_int64, C.c_double, C.c_double, C.c_int32,
                                     _vp, _vp, _vp], C.c_int),
+    "mdb_nph_protocol_from_config": ([_cfgp, C.POINTER(MDBNphProtocol)], C.c_int),
+    "mdb_sim_run_nph_protocol": ([_vp, C.POINTER(MDBNphProtocol), C.POINTER(MDBNphRecord),
+                                  C.c_int64, C.POINTER(MDBNphResult)], C.c_int),
+    "mdb_nph_protocol_dry_run": ([C.POINTER(MDBNphProtocol), _dp, C.c_int64,
+                                  C.POINTER(MDBNphRecord), C.c_int64, C.POINTER(MDBNphResult),
+                                  C.POINTER(C.c_int64)], C.c_int),
     "mdb_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
     "mdb_version": ([], C.c_char_p),
     "mdb_kernel_launches": ([], C.c_int64),
