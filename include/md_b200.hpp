@@ -237,6 +237,17 @@ class MDSimulation {
     check(mdb_sim_create_from_pframe(&c, filename.c_str(), (uint64_t)step, &opt, &sim_),
           "MDSimulation(file)");
   }
+  // Restart from a checkpoint (frame `step` of `filename` + its state file).
+  template <class Comm>
+  MDSimulation(MDConfigManager config_manager, Comm /*ignored*/, const std::string& filename,
+               int step, const std::string& state_file,
+               const mdb_options_t& opt = default_options())
+      : cfg_manager(std::move(config_manager)) {
+    const mdb_config_t c = cfg_manager.config.to_c();
+    check(mdb_sim_create_from_checkpoint(&c, filename.c_str(), (uint64_t)step,
+                                         state_file.c_str(), &opt, &sim_),
+          "MDSimulation(checkpoint)");
+  }
   // A frame given directly (what the ctor-from-file does after reading it).
   MDSimulation(MDConfigManager config_manager, const std::vector<Particle>& frame,
                const mdb_options_t& opt = default_options())
@@ -318,6 +329,28 @@ class MDSimulation {
   }
   void save_env(const std::string& filename, const int step) {
     check(mdb_sim_save_pframe(sim_, filename.c_str(), (uint64_t)step), "save_env");
+  }
+
+  // save_env plus the integrator state (restore with the checkpoint constructor)
+  void save_checkpoint(const std::string& filename, int step, const std::string& state_file) {
+    check(mdb_sim_save_checkpoint(sim_, filename.c_str(), (uint64_t)step, state_file.c_str()),
+          "save_checkpoint");
+  }
+  // The protocol of tests/run_NPH_test/run_test_NPH.cpp (parameters from the
+  // configuration); records receive the per-sample log.
+  mdb_nph_result_t run_nph_protocol(std::vector<mdb_nph_record_t>* records = nullptr) {
+    mdb_nph_protocol_t q;
+    const mdb_config_t c = cfg_manager.config.to_c();
+    check(mdb_nph_protocol_from_config(&c, &q), "run_nph_protocol");
+    std::vector<mdb_nph_record_t> buf(records ? 1 << 16 : 0);
+    mdb_nph_result_t r;
+    check(mdb_sim_run_nph_protocol(sim_, &q, buf.data(), (int64_t)buf.size(), &r),
+          "run_nph_protocol");
+    if (records) {
+      buf.resize((size_t)(r.n_records < (int64_t)buf.size() ? r.n_records : (int64_t)buf.size()));
+      records->swap(buf);
+    }
+    return r;
   }
 
   mdb_observables_t observables() const { return obs(); }

@@ -96,6 +96,14 @@ int main(int argc, char** argv) {
              back[i].vel.x == frame[i].vel.x && back[i].type == frame[i].type;
     expect(same, "save_env + constructor from file");
 
+    std::vector<double> prof = again.get_pressure_profile(8);
+    expect(prof.size() == 24 && std::isfinite(prof[0]), "get_pressure_profile");
+    std::vector<int> counts = again.get_N_profile(8);
+    int total = 0;
+    for (int c : counts) total += c;
+    expect(total == cm.config.n_particles_global, "get_N_profile counts every particle");
+    expect(std::isfinite(again.cal_partial_U_lambda(0.01)), "cal_partial_U_lambda");
+
     bool threw = false;
     try {
       MDConfigManager bad = cm;
