@@ -223,6 +223,14 @@ typedef struct mdb_observables {
   int32_t nonfinite;              /* 1 when NaN/Inf was seen in the state   */
 } mdb_observables_t;
 int mdb_sim_observables(mdb_sim_t* sim, mdb_observables_t* out);
+/* The same record, queued on the handle's stream after the steps issued so
+ * far, without waiting (no counterpart in the reference, whose getters read
+ * host copies after a device synchronisation): *out is written when the
+ * stream reaches the copy, so it is valid after mdb_sim_synchronize (or any
+ * synchronous call). For a copy that overlaps with computation, *out should
+ * be pinned host memory; any host memory works. An error state is reported by
+ * the next synchronous call. */
+int mdb_sim_observables_async(mdb_sim_t* sim, mdb_observables_t* out);
 
 /* sample_collect + get_host_particles (src/md_env.cu:2502-2514): the frame in
  * the caller's original particle order. n must equal the particle count. */

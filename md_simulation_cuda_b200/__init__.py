@@ -257,6 +257,11 @@ class MDSimulation:
     def cal_instant_pressure(self) -> float:
         return self._scalar(lib().mdb_sim_instant_pressure)
 
+    def observables_async(self, out_ptr: int) -> None:
+        """Queue the observables record into host memory at out_ptr (an
+        MDBObservables-sized buffer, ideally pinned); valid after synchronize()."""
+        check(lib().mdb_sim_observables_async(self._h, C.c_void_p(out_ptr)))
+
     def observables(self) -> MDBObservables:
         o = MDBObservables()
         check(lib().mdb_sim_observables(self._h, C.byref(o)))

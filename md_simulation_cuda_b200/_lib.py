@@ -262,6 +262,7 @@ SIGNATURES = {
     "mdb_sim_density_profile": ([_vp, C.c_int32, _dp], C.c_int),
     "mdb_sim_pressure_profile": ([_vp, C.c_int32, _dp], C.c_int),
     "mdb_sim_observables": ([_vp, C.POINTER(MDBObservables)], C.c_int),
+    "mdb_sim_observables_async": ([_vp, _vp], C.c_int),
     "mdb_sim_get_frame": ([_vp, _vp, C.c_int64], C.c_int),
     "mdb_sim_set_frame": ([_vp, _vp, C.c_int64], C.c_int),
     "mdb_sim_save_pframe": ([_vp, C.c_char_p, C.c_uint64], C.c_int),

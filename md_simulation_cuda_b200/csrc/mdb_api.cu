@@ -330,6 +330,11 @@ int mdb_sim_observables(mdb_sim_t* sim, mdb_observables_t* out) {
   return check_status(sim);
 }
 
+int mdb_sim_observables_async(mdb_sim_t* sim, mdb_observables_t* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  return sim->eng->observables_async(0, sim->t, sim->piston_active ? 1 : 0, out);
+}
+
 int mdb_sim_get_frame(mdb_sim_t* sim, mdb_particle_t* out, int64_t n) {
   if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
   if (n != sim->eng->n(0)) return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the particle count");

@@ -292,6 +292,8 @@ int Engine::build() {
   {
     int rc2 = alloc(&d_aos_, sizeof(mdb_particle_t) * (size_t)maxn);
     if (rc2) return rc2;
+    rc2 = alloc(&d_obs_, sizeof(mdb_observables_t));
+    if (rc2) return rc2;
   }
 #undef MDB_ALLOC
   D.nsys = ns;
@@ -666,6 +668,17 @@ int Engine::profiles(int s, int nb, bool py, double* ptens, int32_t* counts) {
   if (e != cudaSuccess) return cuda_error(e, "profiles");
   if (ptens)
     for (size_t k = 0; k < acc.size(); ++k) ptens[k] = (double)acc[k] / kProfileFix;
+  return MDB_OK;
+}
+
+int Engine::observables_async(int s, double t, int piston_active, mdb_observables_t* host) {
+  MDB_CUDA(cudaSetDevice(device_));
+  k_observables<<<1, 1, 0, stream_>>>(dev_, s, t, piston_active, (mdb_observables_t*)d_obs_);
+  MDB_CUDA(cudaGetLastError());
+  launches_ += 1;
+  count_launches(1);
+  MDB_CUDA(cudaMemcpyAsync(host, d_obs_, sizeof(mdb_observables_t), cudaMemcpyDeviceToHost,
+                           stream_));
   return MDB_OK;
 }
 

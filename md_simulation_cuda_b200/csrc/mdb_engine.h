@@ -67,6 +67,9 @@ class Engine {
   // `host` on the engine's stream and returns without waiting; `host` should
   // be pinned memory for the copy to be asynchronous.
   int export_async(int s, mdb_particle_t* host);
+  // Queues the observables of system s (time t and the piston flag come from
+  // the caller) into `host` on the engine's stream; does not wait.
+  int observables_async(int s, double t, int piston_active, mdb_observables_t* host);
   // Per-type x-bin counts (2*nb ints) and unnormalised Irving-Kirkwood sums
   // in y bins (3*nb doubles: xx | yy | xy) of system s; py selects the y
   // convention of the engine's current cell binning.
@@ -112,6 +115,7 @@ class Engine {
   int scan_grid_ = 0;
   int64_t aos_cap_ = 0;
   void* d_aos_ = nullptr;
+  void* d_obs_ = nullptr;  // one mdb_observables_t staging slot
   std::vector<void*> allocs_;
   std::map<std::tuple<int, int, int, int, int>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
   long long launches_ = 0;

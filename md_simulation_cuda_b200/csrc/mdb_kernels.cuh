@@ -1485,6 +1485,30 @@ __global__ void k_export(Dev D, DevParticle* __restrict__ out, int64_t p0, int64
   }
 }
 
+// mdb_sim_observables of system s from its device state into a staging slot.
+__global__ void k_observables(Dev D, int s, double t, int piston_active,
+                              mdb_observables_t* out) {
+  const SysParams& P = D.sp[s];
+  const SysState& S = D.st[s];
+  mdb_observables_t o;
+  memset(&o, 0, sizeof(o));
+  o.t = t;
+  o.Lx = S.Lx;
+  o.Ly = S.Ly;
+  o.xi = S.xi;
+  o.last_instant_pressure = S.last_P;
+  o.nph_area_momentum = S.pA;
+  o.nph_area_rate = S.pA / P.W;
+  o.nph_piston_velocity = S.vp;
+  o.nph_piston_force = S.Fp;
+  o.n = P.n;
+  o.steps = S.steps;
+  o.rebuilds = S.rebuilds;
+  o.piston_mode_active = piston_active;
+  o.nonfinite = S.nonfinite;
+  *out = o;
+}
+
 // Rebuild flag for every system (creation, frame import, mode switches).
 __global__ void k_force_rebuild(Dev D, int periodic_y) {
   for (int s = threadIdx.x; s < D.nsys; s += blockDim.x) {

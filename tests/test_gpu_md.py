@@ -192,3 +192,31 @@ def test_rebuild_stress(built):
     o = sim.observables()
     assert o.rebuilds > 10
     assert rel_err(sim.cal_total_U(), orc.total_U()) < 1e-5
+
+
+def test_observables_async_matches_sync(built):
+    """mdb_sim_observables_async delivers, per step and without waiting, the
+    record mdb_sim_observables returns."""
+    import ctypes
+
+    import torch
+
+    from md_simulation_cuda_b200 import _lib
+
+    f, cfg = wl.nve_4096(seed=6)
+    sim = mdb.MDSimulation(cfg, frame=f)
+    size = ctypes.sizeof(_lib.MDBObservables)
+    ring = torch.zeros(5 * size, dtype=torch.uint8, pin_memory=True)
+    sync = []
+    for k in range(5):
+        sim.step_single_nose_hoover(nsteps=3)
+        sim.observables_async(ring.data_ptr() + k * size)
+    sim.synchronize()
+    ref = mdb.MDSimulation(cfg, frame=f)
+    for k in range(5):
+        ref.step_single_nose_hoover(nsteps=3)
+        sync.append(ref.observables())
+    for k in range(5):
+        a = _lib.MDBObservables.from_address(ring.data_ptr() + k * size)
+        b = sync[k]
+        assert (a.t, a.Lx, a.Ly, a.xi, a.n, a.steps) == (b.t, b.Lx, b.Ly, b.xi, b.n, b.steps)
