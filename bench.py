@@ -501,7 +501,7 @@ def run_ours(args):
         cpu = cpu_cell_baseline(f, cfg, mode)
 
     # ---- end to end through the C ABI with host buffers ----------------------
-    K2 = max(10, args.steps // 2)
+    K2 = max(10, args.steps)
     pinned = torch.empty(N * 64, dtype=torch.uint8, pin_memory=True)
     host = pinned.numpy().view(mdb.PARTICLE_DTYPE)
     host[:] = f
