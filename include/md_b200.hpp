@@ -321,11 +321,17 @@ class MDSimulation {
   double get_t() const { return obs().t; }
   double get_xi() const { return obs().xi; }
 
-  // The frame is read from the device on demand; sample_collect only waits.
-  void sample_collect() { check(mdb_sim_synchronize(sim_), "sample_collect"); }
-  void get_host_particles(std::vector<Particle>& out) const {
-    out.resize((size_t)obs().n);
-    check(mdb_sim_get_frame(sim_, as_c(out.data()), (int64_t)out.size()), "get_host_particles");
+  // sample_collect gathers the frame to the host (src/md_env.cu:2502-2506);
+  // get_host_particles returns the last gathered frame (:2508-2514), the
+  // current one if nothing was gathered yet.
+  void sample_collect() {
+    host_.resize((size_t)obs().n);
+    check(mdb_sim_get_frame(sim_, as_c(host_.data()), (int64_t)host_.size()), "sample_collect");
+    collected_ = true;
+  }
+  void get_host_particles(std::vector<Particle>& out) {
+    if (!collected_) sample_collect();
+    out = host_;
   }
   void save_env(const std::string& filename, const int step) {
     check(mdb_sim_save_pframe(sim_, filename.c_str(), (uint64_t)step), "save_env");
@@ -370,6 +376,8 @@ class MDSimulation {
     return o;
   }
   mdb_sim_t* sim_ = nullptr;
+  std::vector<Particle> host_;
+  bool collected_ = false;
 };
 
 // FireParams (include/md_energy_minimizer.hpp:11-25).

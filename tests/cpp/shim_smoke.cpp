@@ -89,6 +89,7 @@ int main(int argc, char** argv) {
     sim.save_env(argv[2], 7);
     MDSimulation again(cm, comm, argv[2], 7);
     std::vector<Particle> back;
+    again.sample_collect();
     again.get_host_particles(back);
     bool same = back.size() == frame.size();
     for (size_t i = 0; same && i < frame.size(); ++i)
