@@ -151,11 +151,11 @@ class MDSimulation:
     def __init__(self, config_manager, comm=None, filename: Optional[str] = None,
                  step: Optional[int] = None, *, frame=None, device: int = 0,
                  skin: Optional[float] = None, use_graphs: bool = True,
-                 state_file: Optional[str] = None):
+                 state_file: Optional[str] = None, max_neighbors: Optional[int] = None):
         self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
             else MDConfigManager(_config_of(config_manager))
         self._h = C.c_void_p()
-        opt = options(device, skin, use_graphs)
+        opt = options(device, skin, use_graphs, max_neighbors)
         cfg = self.cfg_manager.config
         if state_file is not None:
             # a checkpoint: frame `step` of `filename` plus the integrator state
@@ -744,14 +744,15 @@ class Server:
 
 
 def compute_forces(config, frame, Lx: float, Ly: float, periodic_y: bool = True,
-                   device: int = 0, skin: Optional[float] = None):
+                   device: int = 0, skin: Optional[float] = None,
+                   max_neighbors: Optional[int] = None):
     """One force evaluation: (acc[n,2], U, W)."""
     f = _as_frame(frame)
     n = len(f)
     acc = np.zeros((n, 2))
     U = C.c_double()
     W = C.c_double()
-    opt = options(device, skin)
+    opt = options(device, skin, True, max_neighbors)
     check(lib().mdb_compute_forces(C.byref(_config_of(config)), frame_ptr(f), n, float(Lx),
                                    float(Ly), 1 if periodic_y else 0, C.byref(opt),
                                    acc.ctypes.data_as(C.POINTER(C.c_double)), C.byref(U),
