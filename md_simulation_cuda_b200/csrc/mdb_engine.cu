@@ -122,7 +122,6 @@ int Engine::build() {
   // MDB_ITEMS=<k> fixes the particles per thread (tuning aid; 0 = automatic).
   const char* items_env = getenv("MDB_ITEMS");
   const int items_fixed = items_env ? atoi(items_env) : 0;
-  int g0 = 0;
   for (int s = 0; s < ns; ++s) {
     const SystemSpec& sp = specs_[s];
     const mdb_config_t& c = sp.cfg;
@@ -137,8 +136,6 @@ int Engine::build() {
                   : (int)std::min<int64_t>(16, std::max<int64_t>(1, (n + wave - 1) / wave));
     P.nb = (n + kThreads * P.items - 1) / (kThreads * P.items);
     P.b0 = b0;
-    P.g0 = g0;
-    g0 += (P.nb + kGroup - 1) / kGroup;
     P.kind = sp.kind;
     P.sig[0] = c.SIGMA_AA;
     P.sig[1] = c.SIGMA_BB;
@@ -284,10 +281,6 @@ int Engine::build() {
   MDB_ALLOC(D.scan_part, ntiles + 1);
   MDB_ALLOC(D.part, (int64_t)nblocks_ * kNP);
   MDB_ALLOC(D.partm, (int64_t)nblocks_ * 4);
-  MDB_ALLOC(D.gpart, (int64_t)g0 * kNP);
-  MDB_ALLOC(D.gpartm, (int64_t)g0 * 4);
-  MDB_ALLOC(D.gcount, g0);
-  ngroups_ = g0;
   aos_cap_ = maxn;
   {
     int rc2 = alloc(&d_aos_, sizeof(mdb_particle_t) * (size_t)maxn);
@@ -327,7 +320,6 @@ int Engine::build() {
   MDB_CUDA(cudaMemcpyAsync(D.bg, &bg, sizeof(bg), cudaMemcpyHostToDevice, stream_));
   MDB_CUDA(cudaMemsetAsync(D.part, 0, sizeof(double) * (size_t)nblocks_ * kNP, stream_));
   MDB_CUDA(cudaMemsetAsync(D.partm, 0, sizeof(double) * (size_t)nblocks_ * 4, stream_));
-  MDB_CUDA(cudaMemsetAsync(D.gcount, 0, sizeof(uint32_t) * (size_t)ngroups_, stream_));
   MDB_CUDA(cudaMemsetAsync(D.cell_of, 0, sizeof(int32_t) * (size_t)ntot_, stream_));
   MDB_CUDA(cudaStreamSynchronize(stream_));
   built_ = true;

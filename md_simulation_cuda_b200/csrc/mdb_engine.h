@@ -110,7 +110,6 @@ class Engine {
   Dev dev_{};
   int64_t ntot_ = 0, ncells_ = 0;
   int nblocks_ = 0;
-  int ngroups_ = 0;
   int rb_grid_ = 0;
   int scan_grid_ = 0;
   int64_t aos_cap_ = 0;

@@ -26,7 +26,6 @@ constexpr int kNP = 6;         // reduction slots per block
 constexpr int kScanItems = 4;  // cells per thread in the scan kernels
 constexpr int kScanBlock = 512;
 constexpr int kScanTile = kScanItems * kScanBlock;
-constexpr int kGroup = 64;     // blocks per first-level reduction group
 // ncount[] flag: the list needs neither the minimum image nor offset wrapping.
 constexpr int32_t kListInterior = 1 << 30;
 
@@ -54,7 +53,6 @@ struct SysParams {
   int32_t b0;     // first block of the block table
   int32_t nb;     // blocks
   int32_t items;  // particles per thread (a block covers kThreads*items slots)
-  int32_t g0;     // first reduction group (groups of kGroup blocks)
   int32_t ccap_x, ccap_y;
   int32_t kind;
   float frl2[3];  // neighbour-list radius^2 per pair class: (rc_ij + skin)^2
@@ -134,9 +132,6 @@ struct Dev {
   int32_t* scan_part; // per scan tile
   double* part;       // nblocks * kNP   block partial sums
   double* partm;      // nblocks * 4     block partial maxima
-  double* gpart;      // ngroups * kNP   group partial sums
-  double* gpartm;     // ngroups * 4     group partial maxima
-  uint32_t* gcount;   // ngroups         group arrival counters
   int32_t nsys;
   int32_t nblocks;
   int64_t ntot;

@@ -134,21 +134,19 @@ __device__ __forceinline__ void block_reduce(double (&s)[kNP], double (&m)[3]) {
 
 // Sums (and maxima) of one value set over the blocks of a system, without a
 // second launch and independent of block timing: each block publishes its
-// partials; the last block of every group of kGroup blocks sums that group in
-// a fixed order; the last group to finish sums the group partials in a fixed
-// order. Returns true in that final block, whose thread 0 then holds the
-// system totals in tot/tmx. red/mx hold the calling thread's contributions.
+// partials and counts itself in with one acquire-release atomic (the release
+// publishes its partials, the acquire makes every earlier block's visible);
+// the block that arrives last sums all partials of the system in a fixed
+// order (thread t takes blocks t, t + kThreads, ..., then the block tree).
+// Returns true in that final block, whose thread 0 then holds the system
+// totals in tot/tmx; its thread 0 resets S->counter when it is done.
+// red/mx hold the calling thread's contributions.
 template <int NS, int NM>
 __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, SysState* S,
                                               double (&red)[kNP], double (&mx)[3],
                                               double (&tot)[kNP], double (&tmx)[3]) {
-  __shared__ int sh_last_group, sh_last_system;
+  __shared__ int sh_last;
   block_reduce<NS, NM>(red, mx);
-  const int lb = (int)blockIdx.x - P.b0;
-  const int g = lb / kGroup;
-  const int gsize = min(kGroup, P.nb - g * kGroup);
-  const int ng = (P.nb + kGroup - 1) / kGroup;
-  const int gg = P.g0 + g;
   if (threadIdx.x == 0) {
     double* p = D.part + (size_t)blockIdx.x * kNP;
 #pragma unroll
@@ -156,52 +154,25 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
     double* pm = D.partm + (size_t)blockIdx.x * 4;
 #pragma unroll
     for (int k = 0; k < NM; ++k) pm[k] = mx[k];
-    __threadfence();
-    const unsigned prev = atomicAdd(D.gcount + gg, 1u);
-    sh_last_group = (prev == (unsigned)(gsize - 1)) ? 1 : 0;
+    unsigned prev;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                 : "=r"(prev)
+                 : "l"(&S->counter)
+                 : "memory");
+    sh_last = (prev == (unsigned)(P.nb - 1)) ? 1 : 0;
   }
   __syncthreads();
-  if (!sh_last_group) return false;
-  __threadfence();
-  double s[kNP];
-  double m[3];
-#pragma unroll
-  for (int k = 0; k < kNP; ++k) s[k] = 0.0;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) m[k] = 0.0;
-  if ((int)threadIdx.x < gsize) {
-    const size_t blk = (size_t)(P.b0 + g * kGroup + threadIdx.x);
-#pragma unroll
-    for (int k = 0; k < NS; ++k) s[k] = __ldcg(D.part + blk * kNP + k);
-#pragma unroll
-    for (int k = 0; k < NM; ++k) m[k] = __ldcg(D.partm + blk * 4 + k);
-  }
-  block_reduce<NS, NM>(s, m);
-  if (threadIdx.x == 0) {
-    double* p = D.gpart + (size_t)gg * kNP;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) p[k] = s[k];
-    double* pm = D.gpartm + (size_t)gg * 4;
-#pragma unroll
-    for (int k = 0; k < NM; ++k) pm[k] = m[k];
-    D.gcount[gg] = 0u;
-    __threadfence();
-    const unsigned prev = atomicAdd(&S->counter, 1u);
-    sh_last_system = (prev == (unsigned)(ng - 1)) ? 1 : 0;
-  }
-  __syncthreads();
-  if (!sh_last_system) return false;
-  __threadfence();
+  if (!sh_last) return false;
 #pragma unroll
   for (int k = 0; k < kNP; ++k) tot[k] = 0.0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) tmx[k] = 0.0;
-  for (int q = threadIdx.x; q < ng; q += kThreads) {
-    const size_t gq = (size_t)(P.g0 + q);
+  for (int q = threadIdx.x; q < P.nb; q += kThreads) {
+    const size_t blk = (size_t)(P.b0 + q);
 #pragma unroll
-    for (int k = 0; k < NS; ++k) tot[k] += __ldcg(D.gpart + gq * kNP + k);
+    for (int k = 0; k < NS; ++k) tot[k] += __ldcg(D.part + blk * kNP + k);
 #pragma unroll
-    for (int k = 0; k < NM; ++k) tmx[k] = fmax(tmx[k], __ldcg(D.gpartm + gq * 4 + k));
+    for (int k = 0; k < NM; ++k) tmx[k] = fmax(tmx[k], __ldcg(D.partm + blk * 4 + k));
   }
   block_reduce<NS, NM>(tot, tmx);
   return true;
@@ -218,8 +189,13 @@ struct ForceRed {
 
 // Counts finished systems; the last one sets the graph condition for the
 // rebuild body from the batch-wide flag. Called by thread 0 of a system's
-// last block after its own state is final.
-__device__ __forceinline__ void system_done_and_signal(const Dev& D) {
+// last block after its own state is final. A lone system sets the condition
+// at once from `any` (its own request or one made before this launch).
+__device__ __forceinline__ void system_done_and_signal(const Dev& D, int any) {
+  if (D.nsys == 1) {
+    if (D.use_cond) cudaGraphSetConditional(D.cond, any ? 1u : 0u);
+    return;
+  }
   __threadfence();
   const unsigned prev = atomicAdd(&D.bg->sys_counter, 1u);
   if (prev == (unsigned)(D.nsys - 1)) {
@@ -526,13 +502,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   const double Lx = S->Lx, Ly = S->Ly;
   const double dt = P.dt, h = 0.5 * dt;
   const int items = P.items;
-  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * items + threadIdx.x;
+  // Block b of the system takes the kThreads-slot chunks b, b + nb, b + 2 nb,
+  // ...: the chunks of one block come from across the whole system, so dense
+  // and sparse regions (different list lengths) even out between blocks.
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+  const int64_t stride = (int64_t)P.nb * kThreads;
   const int64_t end = P.p0 + P.n;
   const double xi2 = (FM == FM_NH) ? S->xi : 0.0;
   const double fdt = (FM == FM_FIRE) ? S->f_dt : 0.0;
 #pragma unroll 1
   for (int it = 0; it < items; ++it) {
-    const int64_t i = base + (int64_t)it * kThreads;
+    const int64_t i = base + (int64_t)it * stride;
     if (skip || i >= end) break;
     const int ti = D.type[i];
     double fx, fy, w, u, an;
@@ -866,6 +846,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   double tmx[3];
   if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
+  int need = 0;
+  // a request made before this launch (a forced rebuild)
+  const int prior = (D.nsys == 1) ? *((volatile int*)&D.bg->any_rebuild) : 0;
   if (!skip) {
     if (boxbad) {
       S->err = 5;  // MDB_ERR_BOX
@@ -896,7 +879,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
       const double fy = (DMd == DM_PISTON) ? 1.0 : Ly / S->Ly_b;
       const double f = fmin(fx, fy);
       const double dmax = sqrt(tmx[0] * tmx[0] + tmx[1] * tmx[1]);
-      int need = 0;
       if (!S->allpairs) {
         if (2.0 * tmx[0] + slop + P.rc_max >= wx) need = 1;
         if (2.0 * tmx[1] + slop + P.rc_max >= wy) need = 1;
@@ -912,7 +894,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
     }
   }
   S->counter = 0u;
-  system_done_and_signal(D);
+  system_done_and_signal(D, prior | need);
 }
 
 // K = sum 1/2 m |v|^2 (cal_local_K_kernel src/md_cuda_common.cu:554-589) into
