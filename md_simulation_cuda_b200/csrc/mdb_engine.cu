@@ -117,8 +117,11 @@ int Engine::build() {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
   // A block covers kThreads * items slots of one system; large systems take
   // several particles per thread so that one wave of ~4 blocks per SM covers
-  // them (fewer block partials, a short reduction tail).
+  // them: every block is resident from the start (the force phase spreads
+  // each block's chunks over the system, which balances only within a wave),
+  // fewer block partials, a short reduction tail.
   const int64_t wave = (int64_t)nsm * 4 * kThreads;
+  constexpr int kMaxItems = 4096;
   // MDB_ITEMS=<k> fixes the particles per thread (tuning aid; 0 = automatic).
   const char* items_env = getenv("MDB_ITEMS");
   const int items_fixed = items_env ? atoi(items_env) : 0;
@@ -132,8 +135,8 @@ int Engine::build() {
     P.p0 = p0;
     P.n = n;
     P.items = items_fixed > 0
-                  ? std::min(items_fixed, 16)
-                  : (int)std::min<int64_t>(16, std::max<int64_t>(1, (n + wave - 1) / wave));
+                  ? std::min(items_fixed, kMaxItems)
+                  : (int)std::min<int64_t>(kMaxItems, std::max<int64_t>(1, (n + wave - 1) / wave));
     P.nb = (n + kThreads * P.items - 1) / (kThreads * P.items);
     P.b0 = b0;
     P.kind = sp.kind;
@@ -300,6 +303,22 @@ int Engine::build() {
   scan_grid_ = (int)std::min<int64_t>(ntiles, (int64_t)nsm * 4);
   scan_grid_ = std::max(scan_grid_, 1);
   D.rb_grid = rb_grid_;
+  // The list build is instruction-bound with per-slot costs that vary (list
+  // lengths, minimum-image slots): one wave of resident blocks, grid-stride,
+  // so that no SM is left with a partial second wave.
+  {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_rb_nlist, kThreads,
+                                                      0) != cudaSuccess ||
+        per_sm <= 0) {
+      (void)cudaGetLastError();
+      nlist_grid_ = rb_grid_;
+    } else {
+      nlist_grid_ = (int)std::min<int64_t>((ntot_ + kThreads - 1) / kThreads,
+                                           (int64_t)nsm * per_sm);
+      nlist_grid_ = std::max(nlist_grid_, 1);
+    }
+  }
 
   // block table, per-slot system ids, parameters, state
   std::vector<int32_t> hsob(nblocks_), hsid(ntot_);
@@ -357,7 +376,7 @@ int Engine::launch_rebuild_eager() {
   if ((rc = launch((void*)k_rb_cellsort, rb_grid_, kThreads, d))) return rc;
   if ((rc = launch((void*)k_rb_permute, rb_grid_, kThreads, d))) return rc;
   if ((rc = launch((void*)k_rb_copyback, rb_grid_, kThreads, d))) return rc;
-  if ((rc = launch((void*)k_rb_nlist, rb_grid_, kThreads, d))) return rc;
+  if ((rc = launch((void*)k_rb_nlist, nlist_grid_, kThreads, d))) return rc;
   if ((rc = launch((void*)k_rb_finish, 1, kThreads, d))) return rc;
   return MDB_OK;
 }
@@ -415,7 +434,7 @@ int Engine::add_rebuild_body(cudaGraph_t body, const Dev& d) {
       {(void*)k_scan_tiles, scan_grid_, kScanBlock}, {(void*)k_scan_parts, 1, 1024},
       {(void*)k_scan_add, rb_grid_, kThreads},    {(void*)k_rb_scatter, rb_grid_, kThreads},
       {(void*)k_rb_cellsort, rb_grid_, kThreads}, {(void*)k_rb_permute, rb_grid_, kThreads},
-      {(void*)k_rb_copyback, rb_grid_, kThreads}, {(void*)k_rb_nlist, rb_grid_, kThreads},
+      {(void*)k_rb_copyback, rb_grid_, kThreads}, {(void*)k_rb_nlist, nlist_grid_, kThreads},
       {(void*)k_rb_finish, 1, kThreads},
   };
   cudaGraphNode_t prev = nullptr;

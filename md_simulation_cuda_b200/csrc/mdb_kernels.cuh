@@ -178,6 +178,46 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
   return true;
 }
 
+// Scalars the force phase's last block reads after the system reduction,
+// loaded by thread 0 of every block before it (see DriftTail).
+struct ForceTail {
+  int64_t steps, target_steps;
+  double pA, p_ext, fl, ce, vp, W, f_dt, f_alpha, f_tol, f_inc, f_dt_max, f_dec, f_alpha0;
+  int clamped, f_streak, f_step, f_Nmin;
+};
+template <int FM>
+__device__ __forceinline__ ForceTail force_tail_inputs(const SysParams& P, const SysState* S) {
+  ForceTail t{};
+  if (FM == FM_NPH || FM == FM_PISTON) {
+    t.p_ext = S->p_ext;
+    t.clamped = S->clamped;
+    t.fl = S->fl;
+    t.ce = S->ce;
+  }
+  if (FM == FM_NPH) t.pA = S->pA;
+  if (FM == FM_PISTON) {
+    t.vp = S->vp;
+    t.W = P.W;
+  }
+  if (FM == FM_FIRE) {
+    t.f_dt = S->f_dt;
+    t.f_alpha = S->f_alpha;
+    t.f_streak = S->f_streak;
+    t.f_step = S->f_step;
+    t.f_tol = P.f_tol;
+    t.f_inc = P.f_inc;
+    t.f_dt_max = P.f_dt_max;
+    t.f_dec = P.f_dec;
+    t.f_alpha0 = P.f_alpha0;
+    t.f_Nmin = P.f_Nmin;
+  }
+  if (FM != FM_INIT && FM != FM_OBS && FM != FM_FIRE) {
+    t.steps = S->steps;
+    t.target_steps = P.target_steps;
+  }
+  return t;
+}
+
 // Number of sums / maxima each phase reduces.
 template <int FM>
 struct ForceRed {
@@ -207,14 +247,44 @@ __device__ __forceinline__ void system_done_and_signal(const Dev& D, int any) {
 
 // xi += 0.5 dt (2K - g T0) / Q (src/md_env.cu:1668-1673), host-order
 // arithmetic without contraction.
-__device__ __forceinline__ double nh_xi(const SysParams& P, double xi, double K) {
-  const double t1 = 0.5 * P.dt;
+__device__ __forceinline__ double nh_xi(double dt, double g_dof, double T0, double Q, double xi,
+                                        double K) {
+  const double t1 = 0.5 * dt;
   const double t2 = 2.0 * K;
-  const double t3 = P.g_dof * P.T0;
+  const double t3 = g_dof * T0;
   const double t4 = t2 - t3;
   const double t5 = t1 * t4;
-  const double t6 = t5 / P.Q;
+  const double t6 = t5 / Q;
   return xi + t6;
+}
+__device__ __forceinline__ double nh_xi(const SysParams& P, double xi, double K) {
+  return nh_xi(P.dt, P.g_dof, P.T0, P.Q, xi, K);
+}
+
+// Scalars the drift's last block reads after the system reduction. Thread 0
+// of every block loads them before the reduction: after its acquire every
+// global load is an L2 round trip, and these would be a chain of them.
+struct DriftTail {
+  double g_dof, T0, Q, rc_max, skin, Lx_b, Ly_b;
+  int ncx, ncy, allpairs, prior;
+};
+__device__ __forceinline__ DriftTail drift_tail_inputs(const Dev& D, const SysParams& P,
+                                                       const SysState* S) {
+  DriftTail t;
+  t.g_dof = P.g_dof;
+  t.T0 = P.T0;
+  t.Q = P.Q;
+  t.rc_max = P.rc_max;
+  t.skin = P.skin;
+  t.Lx_b = S->Lx_b;
+  t.Ly_b = S->Ly_b;
+  t.ncx = S->ncx;
+  t.ncy = S->ncy;
+  t.allpairs = S->allpairs;
+  // a rebuild requested before this launch (a forced rebuild); for a lone
+  // system nothing else changes the flag until this block sets it
+  t.prior = (D.nsys == 1) ? *((volatile int*)&D.bg->any_rebuild) : 0;
+  return t;
 }
 
 // --------------------------------------------------------- pair interaction --
@@ -531,7 +601,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       }
       red[5] += an;
     } else {
-      double ax = fx / m, ay = fy / m;
+      // x / 1.0 == x exactly: skip the two FP64 divisions for unit masses
+      double ax, ay;
+      if (m == 1.0) {
+        ax = fx;
+        ay = fy;
+      } else {
+        ax = fx / m;
+        ay = fy / m;
+      }
       if (!PY && (FM == FM_INIT || FM == FM_PISTON)) {
         double up, en;
         const double wf = wall_terms(D.pos[i].y, Ly, P.k_piston, up, en);
@@ -570,20 +648,23 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
     }
   }
   if (bad) atomicOr(&S->nonfinite, 1);
+  ForceTail tin;
+  if (threadIdx.x == 0) tin = force_tail_inputs<FM>(P, S);
   double tot[kNP];
   double tmx[3];
   if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
+  int conv = 0;
   if (!skip) {
     if (FM == FM_NH) {
       S->K = tot[0];
     } else if (FM == FM_NPH) {
       const double A = Lx * Ly;
       const double p_new = (A > 0.0) ? (tot[0] + tot[2]) / (2.0 * A) : 0.0;
-      double pA = S->pA + h * (p_new - S->p_ext);
-      if (S->clamped) {
-        if (Ly <= S->fl && pA < 0.0) pA = 0.0;
-        if (Ly >= S->ce && pA > 0.0) pA = 0.0;
+      double pA = tin.pA + h * (p_new - tin.p_ext);
+      if (tin.clamped) {
+        if (Ly <= tin.fl && pA < 0.0) pA = 0.0;
+        if (Ly >= tin.ce && pA > 0.0) pA = 0.0;
       }
       S->pA = pA;
       S->last_P = p_new;
@@ -591,11 +672,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       S->Wv = tot[2];
     } else if (FM == FM_PISTON) {
       const double Fp = tot[0];
-      const double a_new = (Fp - S->p_ext * Lx) / P.W;
-      double vp = S->vp + h * a_new;
-      if (S->clamped) {
-        if (Ly <= S->fl && vp < 0.0) vp = 0.0;
-        if (Ly >= S->ce && vp > 0.0) vp = 0.0;
+      const double a_new = (Fp - tin.p_ext * Lx) / tin.W;
+      double vp = tin.vp + h * a_new;
+      if (tin.clamped) {
+        if (Ly <= tin.fl && vp < 0.0) vp = 0.0;
+        if (Ly >= tin.ce && vp > 0.0) vp = 0.0;
       }
       S->vp = vp;
       S->Fp = Fp;
@@ -618,35 +699,39 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       const double maxf = (tmx[1] > 0.0) ? __longlong_as_double(0x7ff8000000000000ULL) : tmx[0];
       S->f_power = tot[0];
       S->f_maxf = maxf;
-      if (maxf < P.f_tol) {
+      if (maxf < tin.f_tol) {
+        conv = 1;
         S->f_conv = 1;
-        S->f_conv_step = S->f_step;
+        S->f_conv_step = tin.f_step;
       } else {
         if (tot[0] > 0.0) {
-          S->f_streak += 1;
-          if (S->f_streak > P.f_Nmin) {
-            const double d2 = S->f_dt * P.f_inc;
-            S->f_dt = d2 < P.f_dt_max ? d2 : P.f_dt_max;
-            const double a2 = S->f_alpha * 0.99;
+          const int streak = tin.f_streak + 1;
+          S->f_streak = streak;
+          if (streak > tin.f_Nmin) {
+            const double d2 = tin.f_dt * tin.f_inc;
+            S->f_dt = d2 < tin.f_dt_max ? d2 : tin.f_dt_max;
+            const double a2 = tin.f_alpha * 0.99;
             S->f_alpha = a2 > 0.0 ? a2 : 0.0;
           }
           S->f_zero_v = 0;
         } else {
-          S->f_dt = S->f_dt * P.f_dec;
+          S->f_dt = tin.f_dt * tin.f_dec;
           S->f_streak = 0;
-          S->f_alpha = P.f_alpha0;
+          S->f_alpha = tin.f_alpha0;
           S->f_zero_v = 1;
         }
-        S->f_step += 1;
+        S->f_step = tin.f_step + 1;
       }
     }
     if (FM != FM_INIT && FM != FM_OBS && FM != FM_FIRE) {
-      S->steps += 1;
+      const int64_t steps = tin.steps + 1;
+      S->steps = steps;
       // an MD segment of a batch ends after its target number of steps
-      if (P.target_steps > 0 && S->steps >= P.target_steps) S->done = 1;
+      if (tin.target_steps > 0 && steps >= tin.target_steps) S->done = 1;
     }
   }
-  if (FM == FM_FIRE) S->f_drift = (!skip && !S->f_conv) ? 1 : 0;
+  // (a system that was converged at launch is skipped)
+  if (FM == FM_FIRE) S->f_drift = (!skip && !conv) ? 1 : 0;
   S->counter = 0u;
 }
 
@@ -842,19 +927,19 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
     }
   }
   if (bad) atomicOr(&S->nonfinite, 1);
+  DriftTail tin;
+  if (threadIdx.x == 0) tin = drift_tail_inputs(D, P, S);
   double tot[kNP];
   double tmx[3];
   if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   int need = 0;
-  // a request made before this launch (a forced rebuild)
-  const int prior = (D.nsys == 1) ? *((volatile int*)&D.bg->any_rebuild) : 0;
   if (!skip) {
     if (boxbad) {
       S->err = 5;  // MDB_ERR_BOX
     } else {
       if (DMd == DM_NH) {
-        S->xi = nh_xi(P, xi1, tot[0]);
+        S->xi = nh_xi(dt, tin.g_dof, tin.T0, tin.Q, xi1, tot[0]);
       } else if (DMd == DM_NPH) {
         S->pA = pA1;
         S->aspect = aspect;
@@ -873,17 +958,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
       // box scaled by f since then, a pair outside the list is still outside
       // rc while 2*max displacement < f*skin - max(0, 1-f)*rc_max.
       const double slop = 1e-3 + 4e-7 * fmax(Lx, Ly);
-      const double wx = Lx / (double)S->ncx;
-      const double wy = (DMd == DM_PISTON) ? (S->Ly_b / (double)S->ncy) : Ly / (double)S->ncy;
-      const double fx = Lx / S->Lx_b;
-      const double fy = (DMd == DM_PISTON) ? 1.0 : Ly / S->Ly_b;
+      const double wx = Lx / (double)tin.ncx;
+      const double wy = (DMd == DM_PISTON) ? (tin.Ly_b / (double)tin.ncy) : Ly / (double)tin.ncy;
+      const double fx = Lx / tin.Lx_b;
+      const double fy = (DMd == DM_PISTON) ? 1.0 : Ly / tin.Ly_b;
       const double f = fmin(fx, fy);
       const double dmax = sqrt(tmx[0] * tmx[0] + tmx[1] * tmx[1]);
-      if (!S->allpairs) {
-        if (2.0 * tmx[0] + slop + P.rc_max >= wx) need = 1;
-        if (2.0 * tmx[1] + slop + P.rc_max >= wy) need = 1;
-        if (2.0 * dmax + slop >= f * P.skin - fmax(0.0, 1.0 - f) * P.rc_max) need = 1;
-        if (!(tmx[2] <= P.skin)) need = 1;  // large single-step moves, NaN
+      if (!tin.allpairs) {
+        if (2.0 * tmx[0] + slop + tin.rc_max >= wx) need = 1;
+        if (2.0 * tmx[1] + slop + tin.rc_max >= wy) need = 1;
+        if (2.0 * dmax + slop >= f * tin.skin - fmax(0.0, 1.0 - f) * tin.rc_max) need = 1;
+        if (!(tmx[2] <= tin.skin)) need = 1;  // large single-step moves, NaN
       } else {
         need = (!(tmx[2] <= 0.25 * fmin(Lx, Ly))) ? 1 : 0;
       }
@@ -894,7 +979,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
     }
   }
   S->counter = 0u;
-  system_done_and_signal(D, prior | need);
+  system_done_and_signal(D, tin.prior | need);
 }
 
 // K = sum 1/2 m |v|^2 (cal_local_K_kernel src/md_cuda_common.cu:554-589) into
