@@ -177,11 +177,13 @@ class MDSimulation:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
+            # (no ctypes constructor here: at interpreter exit the module
+            # globals may already be gone)
+            self._h = None
             try:
                 lib().mdb_sim_destroy(h)
             except Exception:
                 pass
-            self._h = C.c_void_p()
 
     def close(self):
         self.__del__()
@@ -520,11 +522,13 @@ class Batch:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
+            # (no ctypes constructor here: at interpreter exit the module
+            # globals may already be gone)
+            self._h = None
             try:
                 lib().mdb_batch_destroy(h)
             except Exception:
                 pass
-            self._h = C.c_void_p()
 
     def add_fire(self, config, frame, force_tol: float, max_steps: int,
                  params: FireParams) -> int:
