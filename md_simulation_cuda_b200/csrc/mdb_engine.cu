@@ -434,8 +434,6 @@ int Engine::add_rebuild_body(cudaGraph_t body, const Dev& d) {
       {(void*)k_scan_tiles, scan_grid_, kScanBlock}, {(void*)k_scan_parts, 1, 1024},
       {(void*)k_scan_add, rb_grid_, kThreads},    {(void*)k_rb_scatter, rb_grid_, kThreads},
       {(void*)k_rb_cellsort, rb_grid_, kThreads}, {(void*)k_rb_permute, rb_grid_, kThreads},
-      {(void*)k_rb_copyback, rb_grid_, kThreads}, {(void*)k_rb_nlist, nlist_grid_, kThreads},
-      {(void*)k_rb_finish, 1, kThreads},
   };
   cudaGraphNode_t prev = nullptr;
   for (const K& k : ks) {
@@ -445,7 +443,17 @@ int Engine::add_rebuild_body(cudaGraph_t body, const Dev& d) {
     if (rc) return rc;
     prev = node;
   }
-  return MDB_OK;
+  // After the permutation, the copy of the sorted FP64 state back into the
+  // primary arrays (memory-bound) and the list build (instruction-bound,
+  // reads only the float-float positions and cells) touch disjoint arrays:
+  // two branches that overlap, joined before the finish kernel.
+  cudaGraphNode_t join[2];
+  int rc = add_kernel_node(body, &prev, 1, (void*)k_rb_copyback, rb_grid_, kThreads, d, &join[0]);
+  if (!rc)
+    rc = add_kernel_node(body, &prev, 1, (void*)k_rb_nlist, nlist_grid_, kThreads, d, &join[1]);
+  cudaGraphNode_t fin;
+  if (!rc) rc = add_kernel_node(body, join, 2, (void*)k_rb_finish, 1, kThreads, d, &fin);
+  return rc;
 }
 
 int Engine::add_cond_rebuild(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,

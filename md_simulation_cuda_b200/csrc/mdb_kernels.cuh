@@ -435,12 +435,14 @@ __device__ __forceinline__ void set_profile_class(PairCtx& c, const SysParams& P
 }
 
 // Sum of pair forces on slot i over its 3x3 cell stencil (or every slot of the
-// system for grids narrower than 3 cells). Returns F in FP64.
+// system for grids narrower than 3 cells). Returns F in FP64. tci receives the
+// type class of slot i, decoded from the sign bits of its float-float
+// position (encode_ff), so the type array is not read.
 template <bool PY, bool ENERGY, bool VIRIAL>
 __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
-                                               int64_t i, int ti, double Lx, double Ly,
-                                               double& fx, double& fy, double& w, double& u,
-                                               double& an) {
+                                               int64_t i, double Lx, double Ly, double& fx,
+                                               double& fy, double& w, double& u, double& an,
+                                               int& tci) {
   PairCtx c;
   const float4 qi = __ldg(D.pff + i);
   c.xih = fabsf(qi.x);
@@ -449,7 +451,7 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   c.yil = qi.w;
   split_box(Lx, c.Lxh, c.Lxl, c.invLx);
   split_box(Ly, c.Lyh, c.Lyl, c.invLy);
-  const int tci = type_class(ti);
+  tci = (int)((__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u));
   c.ts = (tci == 2) ? 99u : (uint32_t)tci;
   const int sc = (tci == 2) ? 2 : tci;
   c.rc2s = P.frc2[sc];
@@ -584,10 +586,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   for (int it = 0; it < items; ++it) {
     const int64_t i = base + (int64_t)it * stride;
     if (skip || i >= end) break;
-    const int ti = D.type[i];
     double fx, fy, w, u, an;
-    particle_force<PY, kEnergy, kVirial>(D, P, *S, i, ti, Lx, Ly, fx, fy, w, u, an);
-    const double m = type_mass(P, ti);
+    int tci;
+    particle_force<PY, kEnergy, kVirial>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an, tci);
+    const double m = (tci == 0) ? P.massA : P.massB;  // type 0 <=> class 0
     double2 v = D.vel[i];
     if (FM == FM_OBS) {
       red[0] += u;
