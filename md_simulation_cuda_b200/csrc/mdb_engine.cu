@@ -483,8 +483,11 @@ int Engine::get_graph(int kind, int dm, int fm, bool py, int chunk, cudaGraphExe
   cudaGraphNode_t prev = nullptr;
   int rc = MDB_OK;
   for (int k = 0; k < chunk && rc == MDB_OK; ++k) {
+    // No reset of the condition at each launch (cudaGraphCondAssignDefault
+    // cost ~4 us per step node): the drift kernel's last block sets it on
+    // every step before the conditional node reads it.
     cudaGraphConditionalHandle h;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
     if (e != cudaSuccess) {
       rc = cuda_error(e, "cudaGraphConditionalHandleCreate");
       break;
