@@ -106,7 +106,8 @@ typedef struct mdb_config {
 /* Engine options with no counterpart in MDConfig (B200 engine knobs). */
 typedef struct mdb_options {
   int32_t device;     /* CUDA device ordinal (default 0)                    */
-  double skin;        /* cell-list skin in sigma units (default 0.3)        */
+  double skin;        /* Verlet-list skin in sigma units; 0 (default):
+                         0.45, or 0.2 when every system is a FIRE run    */
   int32_t use_graphs; /* 1: replay captured CUDA graphs for step chunks     */
   int32_t max_neighbors; /* neighbour-list capacity per particle (default 48;
                             -1: no lists, always scan the cell stencil)     */

@@ -576,7 +576,7 @@ void mdb_options_default(mdb_options_t* out) {
   if (!out) return;
   memset(out, 0, sizeof(*out));
   out->device = 0;
-  out->skin = 0.3;
+  out->skin = 0.0;
   out->use_graphs = 1;
   out->max_neighbors = 48;
 }

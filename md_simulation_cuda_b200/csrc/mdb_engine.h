@@ -100,7 +100,7 @@ class Engine {
   void drop_graphs();
 
   int device_ = 0;
-  double skin_ = 0.3;
+  double skin_ = 0.0;
   int max_nbr_ = 48;
   bool use_graphs_ = true;
   bool built_ = false;

@@ -22,6 +22,8 @@
 namespace mdb {
 
 constexpr int kThreads = 256;  // particle kernels: one particle per thread
+constexpr double kSkinMD = 0.45;   // automatic list skin: MD systems
+constexpr double kSkinFire = 0.2;  // automatic list skin: a handle of FIRE systems only
 constexpr int kNP = 6;         // reduction slots per block
 constexpr int kScanItems = 4;  // cells per thread in the scan kernels
 constexpr int kScanBlock = 512;

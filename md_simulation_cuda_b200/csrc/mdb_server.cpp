@@ -376,7 +376,7 @@ void mdb_server_options_default(mdb_server_options_t* o) {
   o->max_batch_particles = 8 << 20;
   o->max_batch_systems = 1024;
   o->chunk = 500;
-  o->skin = 0.3;
+  o->skin = 0.0;
   o->use_graphs = 1;
   o->max_neighbors = 48;
 }
