@@ -362,7 +362,7 @@ def run_served(args):
            "config": {"workload": f"served stream: {len(specs)} requests, Poisson 200/s, 70% NVT "
                                   "(N log-uniform [1024, 262144], 1000-20000 steps, T ~ U(0.5,1.2)) "
                                   "/ 30% FIRE quench (same N law, tol 1e-6, 20000 its)",
-                      "server": "mdb.Server defaults (8 batches in flight, 80% of free HBM)"},
+                      "server": "mdb.Server defaults (8 batches in flight, 80% of free HBM, least work first, 60 s aging bound)"},
            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                          "max": float(lat.max()),
                          "nvt_p50": float(np.percentile(lat_md, 50)) if len(lat_md) else None,

@@ -437,10 +437,11 @@ int mdb_batch_cuda_stream(mdb_batch_t* b, void** stream);
 /* ---- serving: continuous batching of MD and FIRE requests ------------------
  * No counterpart in the reference (which runs one MPI job per simulation). A
  * server owns one worker thread and one device. Requests (an MD segment or a
- * FIRE quench, each with its own config and frame) wait in a FIFO queue; while
+ * FIRE quench, each with its own config and frame) wait in a queue; while
  * fewer than max_active_batches batches are in flight and the HBM budget
- * allows, the oldest request and the following queued requests of the same
- * kind are admitted together as a new batch on its own stream, so requests
+ * allows, the first request in the admission order (MDB_ORDER_*) and the
+ * following requests of the same kind in that order are admitted together as
+ * a new batch on its own stream, so requests
  * admitted at different times run concurrently. Results (frame and
  * observables) become available as soon as the request's own system
  * finishes; a batch's device memory is released when all of its systems
@@ -459,8 +460,21 @@ typedef struct mdb_server_options {
   double skin;                 /* as mdb_options_t                               */
   int32_t use_graphs;
   int32_t max_neighbors;
-  int32_t reserved[8];
+  int32_t order;               /* admission order (default MDB_ORDER_SHORTEST)  */
+  int32_t max_wait_ms;         /* MDB_ORDER_SHORTEST: requests queued longer
+                                  than this go first, oldest first (default
+                                  60000; 0: no bound)                           */
+  int32_t reserved[6];
 } mdb_server_options_t;
+
+/* Admission order of queued requests. FIFO: the oldest request and the
+ * following queued requests of its kind. SHORTEST: the request with the least
+ * work (particles x steps, or particles x max_steps for FIRE) and the queued
+ * requests of its kind in order of work; a request waiting longer than
+ * max_wait_ms goes before any that has not. Throughput is the same; SHORTEST
+ * lowers the median latency when the queue is long. */
+#define MDB_ORDER_FIFO 0
+#define MDB_ORDER_SHORTEST 1
 
 typedef struct mdb_request {
   int32_t kind;            /* MDB_JOB_FIRE, MDB_JOB_NVE or MDB_JOB_NVT          */

@@ -34,13 +34,15 @@ from ._lib import (MDB_ERR_ARG, MDBConfigC, MDBError, MDBFireParams, MDBMinimize
 # job kinds (mdb200.h MDB_JOB_*) and request states (MDB_REQ_*)
 JOB_FIRE, JOB_NVE, JOB_NVT = 0, 1, 2
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+# server admission orders (MDB_ORDER_*)
+ORDER_FIFO, ORDER_SHORTEST = 0, 1
 
 __all__ = [
     "PARTICLE_DTYPE", "MDBError", "MDConfig", "MDConfigManager", "MDSimulation",
     "EnergyMinimizer", "FireParams", "MinimizeResult", "FileWriter", "FileReader",
     "TrajectoryWriter", "Batch", "Server", "RequestResult", "make_frame", "compute_forces",
     "cell_build", "kernel_launches", "JOB_FIRE", "JOB_NVE", "JOB_NVT", "REQ_QUEUED",
-    "REQ_RUNNING", "REQ_DONE", "REQ_FAILED",
+    "REQ_RUNNING", "REQ_DONE", "REQ_FAILED", "ORDER_FIFO", "ORDER_SHORTEST",
 ]
 
 MDConfig = MDBConfigC  # field-for-field MDConfig
@@ -658,12 +660,16 @@ class Server:
     """Continuous batching of MD segments and FIRE quenches on one GPU
     (mdb_server_*): submit_*() queues a request and returns at once; requests
     are admitted into batches by an HBM budget as slots and memory free up,
-    and run concurrently with the batches already on the device."""
+    and run concurrently with the batches already on the device. `order`:
+    ORDER_SHORTEST (default) admits the queued request with the least work
+    (particles x steps) first, requests queued longer than `max_wait_ms`
+    (default 60 s) ahead of all others; ORDER_FIFO admits oldest first."""
 
     def __init__(self, device: int = 0, max_active_batches: Optional[int] = None,
                  hbm_budget_bytes: Optional[int] = None, max_batch_particles: Optional[int] = None,
                  max_batch_systems: Optional[int] = None, chunk: Optional[int] = None,
-                 skin: Optional[float] = None, use_graphs: bool = True):
+                 skin: Optional[float] = None, use_graphs: bool = True,
+                 order: Optional[int] = None, max_wait_ms: Optional[int] = None):
         self._h = C.c_void_p()
         o = MDBServerOptions()
         lib().mdb_server_options_default(C.byref(o))
@@ -672,7 +678,7 @@ class Server:
                         ("hbm_budget_bytes", hbm_budget_bytes),
                         ("max_batch_particles", max_batch_particles),
                         ("max_batch_systems", max_batch_systems), ("chunk", chunk),
-                        ("skin", skin)):
+                        ("skin", skin), ("order", order), ("max_wait_ms", max_wait_ms)):
             if v is not None:
                 setattr(o, name, v)
         o.use_graphs = 1 if use_graphs else 0

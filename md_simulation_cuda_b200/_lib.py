@@ -157,7 +157,9 @@ class MDBServerOptions(C.Structure):
         ("skin", C.c_double),
         ("use_graphs", C.c_int32),
         ("max_neighbors", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("order", C.c_int32),
+        ("max_wait_ms", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

@@ -2,11 +2,13 @@
 //
 // The reference has no server: each simulation is a separate MPI job
 // (scripts/submit_batches_*.sh). Here one worker thread per server owns the
-// GPU work. Requests wait in a FIFO queue; whenever fewer than
-// max_active_batches batches are in flight and the HBM budget allows, the
-// worker admits the oldest request together with the following queued
-// requests of the same kind (up to max_batch_particles / max_batch_systems)
-// as a new batch on its own CUDA stream. Batches in flight advance in chunks
+// GPU work. Requests wait in a queue; whenever fewer than max_active_batches
+// batches are in flight and the HBM budget allows, the worker admits the
+// first request in the admission order together with the following queued
+// requests of the same kind in that order (up to max_batch_particles /
+// max_batch_systems) as a new batch on its own CUDA stream. The default order
+// is least work first (particles x steps), with requests that waited longer
+// than max_wait_ms ahead of all others; MDB_ORDER_FIFO admits oldest first. Batches in flight advance in chunks
 // issued asynchronously, so the work of requests admitted at different times
 // overlaps on the device. After each chunk the worker records the systems
 // that finished (their frames and observables become results at once), and
@@ -20,6 +22,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -82,6 +85,13 @@ bool valid_config(const mdb_config_t& c, std::string& why) {
     return false;
   }
   return true;
+}
+
+// Work of a request for the shortest-first order: particles x steps (FIRE:
+// the iteration cap).
+double job_work(const Job& j) {
+  const double steps = (j.req.kind == MDB_JOB_FIRE) ? (double)j.req.max_steps : (double)j.req.nsteps;
+  return (double)j.frame.size() * steps;
 }
 
 std::string last_error_text() {
@@ -149,15 +159,26 @@ bool mdb_server::admit() {
   {
     std::lock_guard<std::mutex> lk(mu);
     if (queue.empty() || (int)active.size() >= opt.max_active_batches) return false;
-    const int32_t kind = queue.front()->req.kind;
+    // candidates in admission order (queue order for FIFO)
+    std::vector<JobPtr> order(queue.begin(), queue.end());
+    if (opt.order == MDB_ORDER_SHORTEST) {
+      const double t = now(), wait = 1e-3 * (double)opt.max_wait_ms;
+      auto overdue = [&](const JobPtr& j) {
+        return opt.max_wait_ms > 0 && t - j->res.t_submit > wait;
+      };
+      std::stable_sort(order.begin(), order.end(), [&](const JobPtr& a, const JobPtr& b) {
+        const bool oa = overdue(a), ob = overdue(b);
+        if (oa != ob) return oa;                                 // overdue first,
+        if (oa) return a->res.t_submit < b->res.t_submit;        // oldest first;
+        return job_work(*a) < job_work(*b);                      // then least work
+      });
+    }
+    const int32_t kind = order.front()->req.kind;
     int64_t particles = 0;
-    for (auto it = queue.begin(); it != queue.end();) {
+    for (auto it = order.begin(); it != order.end(); ++it) {
       const JobPtr j = *it;
       const int64_t n = (int64_t)j->frame.size();
-      if (j->req.kind != kind) {
-        ++it;
-        continue;
-      }
+      if (j->req.kind != kind) continue;
       const bool first = group.empty();
       if (!first && ((int)group.size() >= opt.max_batch_systems ||
                      particles + n > opt.max_batch_particles))
@@ -166,7 +187,7 @@ bool mdb_server::admit() {
       if (bytes_in_use + e > budget) {
         if (first && active.empty()) {
           // does not fit even alone on an idle device: fail it
-          queue.erase(it);
+          queue.erase(std::find(queue.begin(), queue.end(), j));
           j->res.status = MDB_REQ_FAILED;
           j->res.error = MDB_ERR_CAPACITY;
           j->res.t_done = now();
@@ -180,9 +201,9 @@ bool mdb_server::admit() {
       group.push_back(j);
       particles += n;
       est = e;
-      it = queue.erase(it);
     }
     if (group.empty()) return false;
+    for (const JobPtr& j : group) queue.erase(std::find(queue.begin(), queue.end(), j));
     const double t = now();
     for (auto& j : group) {
       j->res.status = MDB_REQ_RUNNING;
@@ -379,6 +400,8 @@ void mdb_server_options_default(mdb_server_options_t* o) {
   o->skin = 0.0;
   o->use_graphs = 1;
   o->max_neighbors = 48;
+  o->order = MDB_ORDER_SHORTEST;
+  o->max_wait_ms = 60000;
 }
 
 int mdb_server_create(const mdb_server_options_t* opt, mdb_server_t** out) {
@@ -394,6 +417,8 @@ int mdb_server_create(const mdb_server_options_t* opt, mdb_server_t** out) {
   if (o.max_active_batches <= 0 || o.max_batch_systems <= 0 || o.max_batch_particles <= 0 ||
       o.chunk <= 0)
     return mdb::set_error(MDB_ERR_ARG, "server limits must be positive");
+  if ((o.order != MDB_ORDER_FIFO && o.order != MDB_ORDER_SHORTEST) || o.max_wait_ms < 0)
+    return mdb::set_error(MDB_ERR_ARG, "bad admission order or max_wait_ms");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return mdb::set_error(MDB_ERR_NODEVICE, "no CUDA device available");

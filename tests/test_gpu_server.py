@@ -106,3 +106,32 @@ def test_server_budget_and_errors(built):
         bad = dict(cfg, box_w_global=-1.0)
         with pytest.raises(mdb.MDBError):
             srv.submit_md(bad, f, 10)
+
+
+@pytest.mark.parametrize("order, max_wait_ms, expect", [
+    (mdb.ORDER_SHORTEST, 60000, ["small", "medium", "big"]),  # least work first
+    (mdb.ORDER_SHORTEST, 1, ["big", "small", "medium"]),      # all overdue: oldest first
+    (mdb.ORDER_FIFO, 60000, ["big", "small", "medium"]),
+])
+def test_server_admission_order(built, order, max_wait_ms, expect):
+    """Three requests queued behind a running one, one batch at a time: they
+    start in the admission order (work = particles x steps)."""
+    def job(N, seed):
+        f, Lx, Ly = wl.lattice_frame(N, 0.8, 1.0, 0.65, 0.8, seed=seed, jitter=0.1)
+        return f, wl.config_dict(N, Lx, Ly, dt=0.002, T=0.8)
+    with mdb.Server(chunk=100, max_active_batches=1, max_batch_systems=1, order=order,
+                    max_wait_ms=max_wait_ms) as srv:
+        f, cfg = job(2000, 60)
+        blocker = srv.submit_md(cfg, f, 3000)
+        while srv.stats().running == 0:
+            time.sleep(0.001)
+        ids = {}
+        for name, N, nsteps, seed in [("big", 4000, 600, 61), ("small", 900, 250, 62),
+                                      ("medium", 2000, 400, 63)]:
+            f, cfg = job(N, seed)
+            ids[name] = srv.submit_md(cfg, f, nsteps)
+        assert srv.wait(blocker, timeout=300.0) == mdb.REQ_DONE
+        for rid in ids.values():
+            assert srv.wait(rid, timeout=300.0) == mdb.REQ_DONE
+        starts = {name: srv.result(rid).t_start for name, rid in ids.items()}
+    assert sorted(starts, key=starts.get) == expect
