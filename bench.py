@@ -310,7 +310,8 @@ def run_served(args):
     pool = ThreadPoolExecutor(max_workers=8)
     futures = [pool.submit(wl.served_frame, sp) for sp in specs[:64]]
     nxt = len(futures)
-    srv = mdb.Server(device=0)
+    srv = (mdb.Server(device=0, order=mdb.ORDER_FIFO, priorities=False) if args.server_fifo
+           else mdb.Server(device=0))
     host_t0 = time.perf_counter()  # the server clock starts at creation
     ids = queue.Queue()
     clocks = ClockSampler(0)
@@ -362,7 +363,9 @@ def run_served(args):
            "config": {"workload": f"served stream: {len(specs)} requests, Poisson 200/s, 70% NVT "
                                   "(N log-uniform [1024, 262144], 1000-20000 steps, T ~ U(0.5,1.2)) "
                                   "/ 30% FIRE quench (same N law, tol 1e-6, 20000 its)",
-                      "server": "mdb.Server defaults (8 batches in flight, 80% of free HBM, least work first, 60 s aging bound)"},
+                      "server": ("mdb.Server, 8 batches in flight, 80% of free HBM, " +
+                                 ("oldest first, normal stream priority" if args.server_fifo else
+                                  "least work first with a 60 s aging bound, stream priority by batch work"))},
            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                          "max": float(lat.max()),
                          "nvt_p50": float(np.percentile(lat_md, 50)) if len(lat_md) else None,
@@ -586,6 +589,8 @@ def main():
     ap.add_argument("--to-completion", action="store_true",
                     help="fire_mix: run every system until it converges or hits 20000 its")
     ap.add_argument("--requests", type=int, default=2000, help="served: number of requests")
+    ap.add_argument("--server-fifo", action="store_true",
+                    help="served: oldest-first admission, no stream priorities")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -111,7 +111,11 @@ typedef struct mdb_options {
   int32_t use_graphs; /* 1: replay captured CUDA graphs for step chunks     */
   int32_t max_neighbors; /* neighbour-list capacity per particle (default 48;
                             -1: no lists, always scan the cell stencil)     */
-  int32_t reserved[12];
+  int32_t stream_priority; /* 0 (default): the handle's stream has normal
+                              priority; k > 0: k levels above it (clamped to
+                              the device's range), so its kernels' blocks
+                              are scheduled before those of lower streams   */
+  int32_t reserved[11];
 } mdb_options_t;
 
 /* MDConfig{} value-initialised defaults (include/md_config.hpp:14-75). */
@@ -464,7 +468,11 @@ typedef struct mdb_server_options {
   int32_t max_wait_ms;         /* MDB_ORDER_SHORTEST: requests queued longer
                                   than this go first, oldest first (default
                                   60000; 0: no bound)                           */
-  int32_t reserved[6];
+  int32_t priorities;          /* 1 (default): a batch's stream priority rises
+                                  as its work falls, so the kernels of short
+                                  requests are scheduled ahead of long ones;
+                                  0: every batch at normal priority             */
+  int32_t reserved[5];
 } mdb_server_options_t;
 
 /* Admission order of queued requests. FIFO: the oldest request and the

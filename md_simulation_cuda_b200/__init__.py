@@ -663,13 +663,16 @@ class Server:
     and run concurrently with the batches already on the device. `order`:
     ORDER_SHORTEST (default) admits the queued request with the least work
     (particles x steps) first, requests queued longer than `max_wait_ms`
-    (default 60 s) ahead of all others; ORDER_FIFO admits oldest first."""
+    (default 60 s) ahead of all others; ORDER_FIFO admits oldest first.
+    `priorities` (default on): batches holding less work get higher CUDA
+    stream priority, so short requests' kernels go first."""
 
     def __init__(self, device: int = 0, max_active_batches: Optional[int] = None,
                  hbm_budget_bytes: Optional[int] = None, max_batch_particles: Optional[int] = None,
                  max_batch_systems: Optional[int] = None, chunk: Optional[int] = None,
                  skin: Optional[float] = None, use_graphs: bool = True,
-                 order: Optional[int] = None, max_wait_ms: Optional[int] = None):
+                 order: Optional[int] = None, max_wait_ms: Optional[int] = None,
+                 priorities: Optional[bool] = None):
         self._h = C.c_void_p()
         o = MDBServerOptions()
         lib().mdb_server_options_default(C.byref(o))
@@ -678,7 +681,8 @@ class Server:
                         ("hbm_budget_bytes", hbm_budget_bytes),
                         ("max_batch_particles", max_batch_particles),
                         ("max_batch_systems", max_batch_systems), ("chunk", chunk),
-                        ("skin", skin), ("order", order), ("max_wait_ms", max_wait_ms)):
+                        ("skin", skin), ("order", order), ("max_wait_ms", max_wait_ms),
+                        ("priorities", None if priorities is None else int(bool(priorities)))):
             if v is not None:
                 setattr(o, name, v)
         o.use_graphs = 1 if use_graphs else 0

@@ -99,7 +99,8 @@ class MDBOptions(C.Structure):
         ("skin", C.c_double),
         ("use_graphs", C.c_int32),
         ("max_neighbors", C.c_int32),
-        ("reserved", C.c_int32 * 12),
+        ("stream_priority", C.c_int32),
+        ("reserved", C.c_int32 * 11),
     ]
 
 
@@ -159,7 +160,8 @@ class MDBServerOptions(C.Structure):
         ("max_neighbors", C.c_int32),
         ("order", C.c_int32),
         ("max_wait_ms", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("priorities", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

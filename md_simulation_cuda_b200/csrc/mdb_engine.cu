@@ -50,6 +50,7 @@ Engine::Engine(const mdb_options_t& opt) {
   skin_ = opt.skin > 0.0 ? opt.skin : 0.0;  // 0: chosen at build from the systems' kinds
   use_graphs_ = opt.use_graphs != 0;
   max_nbr_ = opt.max_neighbors > 0 ? opt.max_neighbors : (opt.max_neighbors < 0 ? 0 : 48);
+  stream_priority_ = opt.stream_priority > 0 ? opt.stream_priority : 0;
   // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
   // see kernel nodes of graphs that contain conditional nodes).
   const char* eager = getenv("MDB_EAGER");
@@ -79,7 +80,17 @@ int Engine::ensure_device() {
     return set_error(MDB_ERR_NODEVICE, "no CUDA device available");
   if (device_ < 0 || device_ >= ndev) return set_error(MDB_ERR_ARG, "invalid CUDA device ordinal");
   MDB_CUDA(cudaSetDevice(device_));
-  if (!stream_) MDB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  if (!stream_) {
+    if (stream_priority_ > 0) {
+      // numerically lower is higher priority; "greatest" is the highest
+      int least = 0, greatest = 0;
+      MDB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      const int p = std::max(greatest, least - stream_priority_);
+      MDB_CUDA(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, p));
+    } else {
+      MDB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    }
+  }
   return MDB_OK;
 }
 

@@ -112,7 +112,8 @@ class Engine {
   int nblocks_ = 0;
   int rb_grid_ = 0;
   int scan_grid_ = 0;
-  int nlist_grid_ = 0;  // k_rb_nlist: one wave of resident blocks
+  int nlist_grid_ = 0;
+  int stream_priority_ = 0;  // levels above normal for stream_  // k_rb_nlist: one wave of resident blocks
   int64_t aos_cap_ = 0;
   void* d_aos_ = nullptr;
   void* d_obs_ = nullptr;  // one mdb_observables_t staging slot

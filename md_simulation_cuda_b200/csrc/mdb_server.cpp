@@ -224,6 +224,13 @@ bool mdb_server::admit() {
   o.skin = opt.skin;
   o.use_graphs = opt.use_graphs;
   o.max_neighbors = opt.max_neighbors;
+  if (opt.priorities) {
+    // One stream priority level per decade of batch work (particles x steps):
+    // below 1e9 the highest, 1e12 and above the lowest above normal.
+    double w = 0.0;
+    for (const JobPtr& j : group) w += job_work(*j);
+    o.stream_priority = std::min(5, std::max(1, 13 - (int)floor(log10(std::max(w, 1.0)))));
+  }
   int rc = mdb_batch_create(&o, &ab.b);
   for (size_t k = 0; rc == MDB_OK && k < group.size(); ++k) {
     const Job& j = *group[k];
@@ -402,6 +409,7 @@ void mdb_server_options_default(mdb_server_options_t* o) {
   o->max_neighbors = 48;
   o->order = MDB_ORDER_SHORTEST;
   o->max_wait_ms = 60000;
+  o->priorities = 1;
 }
 
 int mdb_server_create(const mdb_server_options_t* opt, mdb_server_t** out) {
