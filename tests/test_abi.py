@@ -85,3 +85,25 @@ def test_server_needs_a_device(built):
         raise AssertionError("server created without a device")
     except m.MDBError as e:
         assert e.code == _lib.MDB_ERR_NODEVICE
+
+
+def test_server_option_defaults_and_checks(built):
+    """Admission-order and priority options: their defaults, and invalid
+    values rejected before any device work (so this runs without a GPU)."""
+    import ctypes as C
+
+    import md_simulation_cuda_b200 as m
+
+    o = _lib.MDBServerOptions()
+    _lib.lib().mdb_server_options_default(C.byref(o))
+    assert o.order == m.ORDER_SHORTEST and o.max_wait_ms == 60000 and o.priorities == 1
+    assert o.skin == 0.0  # automatic list skin
+    for kw in (dict(order=7), dict(max_wait_ms=-1)):
+        try:
+            m.Server(**kw)
+            raise AssertionError(f"accepted {kw}")
+        except m.MDBError as e:
+            assert e.code == _lib.MDB_ERR_ARG
+    e = _lib.MDBOptions()
+    _lib.lib().mdb_options_default(C.byref(e))
+    assert e.skin == 0.0 and e.stream_priority == 0 and e.max_neighbors == 48
