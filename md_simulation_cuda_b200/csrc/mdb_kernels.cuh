@@ -560,6 +560,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
+  {
+    // L1 prefetch of this thread's first slot and its first list rows
+    const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+    if (i0 < P.p0 + P.n) {
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.pff + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.vel + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.ncount + i0));
+      if (D.nl16 && D.max_nbr >= 8) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(D.nlist16 + (int64_t)q * D.ntot + i0));
+      }
+    }
+  }
   // a finished batch system is still observed (FM_OBS) and re-evaluated (FM_INIT)
   const bool skip = (FM != FM_OBS && FM != FM_INIT && S->done != 0) || (S->err != 0) ||
                     (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
@@ -829,6 +843,18 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
+  {
+    // L1 prefetch of this thread's first particle: its DRAM latency overlaps
+    // the scalar prologue below
+    const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * kThreads * P.items + threadIdx.x;
+    if (i0 < P.p0 + P.n) {
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.pos + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.vel + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.acc + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.type + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.sb + i0));
+    }
+  }
   const bool skip = (S->done != 0) || (S->err != 0) || (DMd == DM_FIRE && S->f_drift == 0);
   constexpr int kNS = (DMd == DM_NH) ? 1 : 0, kNM = 3;
   const double dt = P.dt, h = 0.5 * dt;
