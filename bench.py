@@ -363,7 +363,7 @@ def run_served(args):
            "config": {"workload": f"served stream: {len(specs)} requests, Poisson 200/s, 70% NVT "
                                   "(N log-uniform [1024, 262144], 1000-20000 steps, T ~ U(0.5,1.2)) "
                                   "/ 30% FIRE quench (same N law, tol 1e-6, 20000 its)",
-                      "server": ("mdb.Server, 8 batches in flight, 80% of free HBM, " +
+                      "server": ("mdb.Server, 8 batches in flight of up to 1Mi particles, 80% of free HBM, " +
                                  ("oldest first, normal stream priority" if args.server_fifo else
                                   "least work first with a 60 s aging bound, stream priority by batch work"))},
            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

@@ -458,7 +458,8 @@ typedef struct mdb_server_options {
   int32_t device;              /* CUDA device ordinal (default 0)               */
   int32_t max_active_batches;  /* batches in flight at once (default 8)         */
   int64_t hbm_budget_bytes;    /* device memory for batches (0: 80% of free)    */
-  int64_t max_batch_particles; /* particles per admitted batch (default 8Mi)    */
+  int64_t max_batch_particles; /* particles per admitted batch (default 1Mi; a
+                                  larger request is admitted alone)            */
   int32_t max_batch_systems;   /* systems per admitted batch (default 1024)     */
   int32_t chunk;               /* steps / iterations issued per chunk (500)     */
   double skin;                 /* as mdb_options_t                               */
