@@ -145,6 +145,18 @@ def make_workload(name, rank):
                           "90%/10% A stripes, T=0.7, Q=1.0, dt=0.002")
 
 
+def step_roofline(per_gpu_value, hbm_gbs, p_ord):
+    """The survey's whole-step roofline: particle-steps/s on one GPU against
+    min(HBM bandwidth / 97 B per particle-step, FP32 peak / (24 flops x
+    ordered pairs inside the cutoff per particle))."""
+    bw_bound = hbm_gbs * 1e9 / 97.0
+    fp_bound = FP32_NOMINAL_TFLOPS * 1e12 / (24.0 * p_ord) if p_ord else float("inf")
+    bound = min(bw_bound, fp_bound)
+    return {"achieved": per_gpu_value, "bound": bound, "unit": "particle-steps/s",
+            "limited_by": "hbm" if bw_bound <= fp_bound else "fp32",
+            "frac": per_gpu_value / bound}
+
+
 def cpu_cell_baseline(f, cfg, mode_name, budget_s=20.0):
     """The oracle's cell-list step on all host cores (the fair CPU baseline)."""
     from oracle import pyoracle as po
@@ -564,7 +576,12 @@ def run_ours(args):
                          "fp32": {"achieved_tflops": (24.0 * p_ord * N / t_force / 1e12)
                                   if p_ord else None,
                                   "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_source": "nominal",
-                                  "pairs_per_particle": p_ord}},
+                                  "frac": (24.0 * p_ord * N / t_force / 1e12 / FP32_NOMINAL_TFLOPS)
+                                  if p_ord else None,
+                                  "pairs_per_particle": p_ord},
+                         # whole step: per-GPU particle-steps/s over the step's bound,
+                         # min(HBM peak / 97 B, FP32 peak / (24 flops x P_ord))
+                         "step": step_roofline(value / ws, hbm_peak, p_ord)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
