@@ -210,6 +210,138 @@ int or_forces_allpairs(const or_lj_t* lj, int64_t n, const double* pos, const in
   return 0;
 }
 
+/* ---- the reference's block-reduced kernels, thread by thread -------------- */
+
+/* The pair quantities the reference's pair loops share, in its mixed
+ * arithmetic (src/md_cuda_common.cu:193-249, 616-688, 735-806, 293-361):
+ * FP32 displacement and minimum image, strict FP32 cutoff, FP32 tmp and
+ * u_pair. In FP64 mode the same quantities in double. */
+typedef struct ref_pair {
+  int in, c;
+  double dx, dy, fx, fy, u; /* fx = double(tmp*dx) etc. (exact FP32 values in mixed mode) */
+} ref_pair_t;
+
+static inline ref_pair_t ref_pair_terms(const or_lj_t* lj, int mode, double xi, double yi, int ti,
+                                        double xj, double yj, int tj, double Lx, double Ly,
+                                        int periodic_y) {
+  ref_pair_t r = {0, pair_class(ti, tj), 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (mode == OR_FP64) {
+    double dx = xi - xj, dy = yi - yj;
+    dx = dx - Lx * round(dx / Lx);
+    if (periodic_y) dy = dy - Ly * round(dy / Ly);
+    const double sig = lj->sigma[r.c], eps = lj->epsilon[r.c], rc = lj->cutoff * sig;
+    const double r2 = dx * dx + dy * dy;
+    if (!(r2 > 0.0 && r2 < rc * rc)) return r;
+    const double r2i = 1.0 / r2;
+    const double sr2 = sig * sig * r2i;
+    const double sr6 = sr2 * sr2 * sr2;
+    const double sr12 = sr6 * sr6;
+    const double tmp = 24.0 * eps * (2.0 * sr12 - sr6) * r2i;
+    r.in = 1;
+    r.dx = dx;
+    r.dy = dy;
+    r.fx = tmp * dx;
+    r.fy = tmp * dy;
+    r.u = 4.0 * eps * (sr12 - sr6);
+    return r;
+  }
+  const float Lx_f = (float)Lx, Ly_f = (float)Ly;
+  float dx_f = (float)(xi - xj);
+  float dy_f = (float)(yi - yj);
+  dx_f = fmaf(-Lx_f, roundf(dx_f / Lx_f), dx_f);
+  if (periodic_y) dy_f = fmaf(-Ly_f, roundf(dy_f / Ly_f), dy_f);
+  const float sigma_f = (float)lj->sigma[r.c];
+  const float epsilon_f = (float)lj->epsilon[r.c];
+  const float rc_f = (float)lj->cutoff * sigma_f;
+  const float rc_sq_f = rc_f * rc_f;
+  const float dr_sq_f = fmaf(dx_f, dx_f, dy_f * dy_f);
+  if (!(dr_sq_f > 0.0f && dr_sq_f < rc_sq_f)) return r;
+  const float r2_inv_f = 1.0f / dr_sq_f;
+  const float sr2_f = (sigma_f * sigma_f) * r2_inv_f;
+  const float sr6_f = sr2_f * sr2_f * sr2_f;
+  const float sr12_f = sr6_f * sr6_f;
+  const float tmp_f = (24.0f * epsilon_f) * fmaf(2.0f, sr12_f, -sr6_f) * r2_inv_f;
+  r.in = 1;
+  r.dx = (double)dx_f;
+  r.dy = (double)dy_f;
+  r.fx = (double)(tmp_f * dx_f);
+  r.fy = (double)(tmp_f * dy_f);
+  r.u = (double)((4.0f * epsilon_f) * (sr12_f - sr6_f));
+  return r;
+}
+
+int or_ref_thread_values(const or_lj_t* lj, int64_t n, const double* pos, const double* vel,
+                         const int32_t* type, double Lx, double Ly, int32_t periodic_y,
+                         int32_t mode, int32_t ws1_halo, int32_t what, double eps_lambda,
+                         double* out, int32_t nthreads) {
+  if (!lj || n < 0 || !out || what < OR_SUM_U || what > OR_SUM_DUDL) return 1;
+  if ((what == OR_SUM_P || what == OR_SUM_K) && !vel) return 1;
+  set_threads(nthreads);
+  int64_t* halo = NULL;
+  int64_t nh = 0;
+  if (ws1_halo && what != OR_SUM_K) {
+    halo = (int64_t*)malloc(sizeof(int64_t) * (size_t)(2 * n + 1));
+    if (!halo) return 2;
+    nh = build_ws1_halo(lj, n, pos, Lx, halo);
+  }
+  double vc[3];
+  for (int c = 0; c < 3; ++c) vc[c] = shift_of(lj, c);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < n; ++i) {
+    const int ti = type[i];
+    const double m = type_mass(lj, ti);
+    double acc = 0.0;
+    if (what == OR_SUM_K) {
+      const double vx = vel[2 * i], vy = vel[2 * i + 1];
+      out[i] = (0.5 * m) * fma(vx, vx, vy * vy);
+      continue;
+    }
+    if (what == OR_SUM_P) {
+      const double vx = vel[2 * i], vy = vel[2 * i + 1];
+      acc = m * fma(vx, vx, vy * vy);
+    }
+    const double xi = pos[2 * i], yi = pos[2 * i + 1];
+    for (int64_t q = 0; q < n + nh; ++q) {
+      if (q == i) continue;
+      const int64_t j = q < n ? q : halo[q - n];
+      const ref_pair_t r = ref_pair_terms(lj, mode, xi, yi, ti, pos[2 * j], pos[2 * j + 1],
+                                          type[j], Lx, Ly, periodic_y);
+      if (!r.in) continue;
+      if (what == OR_SUM_U) {
+        acc = fma(0.5, r.u - vc[r.c], acc);
+      } else if (what == OR_SUM_P) {
+        acc = fma(0.5, fma(r.dx, r.fx, r.dy * r.fy), acc);
+      } else {
+        const double pv = -eps_lambda * fma(r.fx, r.dx, -(r.fy * r.dy));
+        acc = fma(0.5, pv, acc);
+      }
+    }
+    out[i] = acc;
+  }
+  free(halo);
+  return 0;
+}
+
+double or_ref_block_partials(int64_t n, const double* v, int32_t threads, double* partials) {
+  if (threads <= 0) threads = 256;
+  double* sh = (double*)malloc(sizeof(double) * (size_t)threads);
+  if (!sh) return NAN;
+  const int64_t nb = (n + threads - 1) / threads;
+  double total = 0.0;
+  for (int64_t b = 0; b < nb; ++b) {
+    for (int32_t t = 0; t < threads; ++t) {
+      const int64_t idx = b * threads + t;
+      sh[t] = idx < n ? v[idx] : 0.0;
+    }
+    for (int32_t s = threads / 2; s > 0; s >>= 1)
+      for (int32_t t = 0; t < s; ++t) sh[t] += sh[t + s];
+    if (partials) partials[b] = sh[0];
+    total += sh[0];
+  }
+  free(sh);
+  return total;
+}
+
 /* ---- project binning ----------------------------------------------------- */
 void or_cell_grid(double Lx, double Ly, double cell_min, int32_t* ncx, int32_t* ncy) {
   double fx = floor(Lx / cell_min);

@@ -83,6 +83,22 @@ int or_n_profile(int64_t n, const double* pos, const int32_t* type, double Lx, i
 int or_pressure_profile(const or_lj_t* lj, int64_t n, const double* pos, const double* vel,
                         const int32_t* type, double Lx, double Ly, int32_t periodic_y,
                         int32_t mode, int32_t nb, double* out);
+/* Per-thread values of the reference's block-reduced kernels, each in its
+ * own accumulation order, with the same halos as or_forces_allpairs:
+ *   OR_SUM_U    cal_local_U_kernel (src/md_cuda_common.cu:703-825)
+ *   OR_SUM_P    cal_local_pressure_scalar_kernel (:591-701), m|v|^2 first
+ *   OR_SUM_K    cal_local_K_kernel (:554-589)
+ *   OR_SUM_DUDL cal_partial_U_lambda_kernel (:266-377) for eps_lambda
+ * out: n doubles (thread i's value before the block reduction). */
+enum { OR_SUM_U = 0, OR_SUM_P = 1, OR_SUM_K = 2, OR_SUM_DUDL = 3 };
+int or_ref_thread_values(const or_lj_t* lj, int64_t n, const double* pos, const double* vel,
+                         const int32_t* type, double Lx, double Ly, int32_t periodic_y,
+                         int32_t mode, int32_t ws1_halo, int32_t what, double eps_lambda,
+                         double* out, int32_t nthreads);
+/* The shared-memory tree of those kernels over blocks of `threads` values
+ * (threads past n add 0): partials[b] (optional), and their sum in block
+ * order as the reference's host loops take it (the return value). */
+double or_ref_block_partials(int64_t n, const double* v, int32_t threads, double* partials);
 /* Ordered in-cutoff pairs counted through a cell list (large systems). */
 int64_t or_count_pairs_cells(const or_lj_t* lj, int64_t n, const double* pos,
                              const int32_t* type, double Lx, double Ly, int32_t nthreads);

@@ -129,6 +129,11 @@ def lib():
             L.or_forces_rows.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, ip, C.c_double,
                                          C.c_double, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                          dp, C.c_int32]
+            L.or_ref_thread_values.argtypes = [C.POINTER(OrLJ), C.c_int64, dp, dp, ip,
+                                               C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                               C.c_int32, C.c_int32, C.c_double, dp, C.c_int32]
+            L.or_ref_block_partials.argtypes = [C.c_int64, dp, C.c_int32, dp]
+            L.or_ref_block_partials.restype = C.c_double
             L.or_cell_grid.argtypes = [C.c_double, C.c_double, C.c_double, ip, ip]
             L.or_cell_bin.argtypes = [C.c_int64, dp, C.c_double, C.c_double, C.c_int32,
                                       C.c_int32, ip]
@@ -263,6 +268,34 @@ def forces_rows(cfg, pos, types, Lx, Ly, row0, nrows, periodic_y=1, mode=OR_REF_
     if rc != 0:
         raise RuntimeError("oracle forces_rows failed")
     return acc
+
+
+OR_SUM_U, OR_SUM_P, OR_SUM_K, OR_SUM_DUDL = 0, 1, 2, 3
+
+
+def ref_thread_values(cfg, pos, vel, types, Lx, Ly, what, periodic_y=1, mode=OR_REF_MIXED,
+                      ws1_halo=0, eps_lambda=0.0, nthreads=0):
+    """Per-thread values of the reference's block-reduced kernels (OR_SUM_*)."""
+    p = _pos2(pos)
+    v = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 2)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    out = np.zeros(p.shape[0])
+    lj = make_lj(cfg)
+    rc = lib().or_ref_thread_values(C.byref(lj), p.shape[0], _dp(p), _dp(v), _ip(t), Lx, Ly,
+                                    periodic_y, mode, ws1_halo, what, float(eps_lambda),
+                                    _dp(out), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle ref_thread_values failed ({rc})")
+    return out
+
+
+def ref_block_partials(values, threads=256):
+    """(block-order total, per-block partials) of the reference's block tree."""
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    nb = (len(v) + threads - 1) // threads
+    part = np.zeros(max(nb, 1))
+    tot = lib().or_ref_block_partials(len(v), _dp(v), threads, _dp(part))
+    return tot, part[:nb]
 
 
 def cell_build(pos, Lx, Ly, cell_min):
