@@ -115,8 +115,20 @@ typedef struct mdb_options {
                               priority; k > 0: k levels above it (clamped to
                               the device's range), so its kernels' blocks
                               are scheduled before those of lower streams   */
-  int32_t reserved[11];
+  int32_t fire_precision; /* FIRE pair arithmetic: MDB_FIRE_AUTO (default)
+                             runs the reference's FP32 pair terms until a
+                             system's max |a| falls below 1e-3, then FP64
+                             pair terms and sums for that system, so that
+                             max |a| < 1e-6 is reachable; MDB_FIRE_FP32 keeps
+                             FP32 pair terms throughout (stalls near 1e-6, as
+                             the reference does); MDB_FIRE_FP64 uses FP64
+                             pair terms from the first iteration           */
+  int32_t reserved[10];
 } mdb_options_t;
+
+#define MDB_FIRE_AUTO 0
+#define MDB_FIRE_FP32 1
+#define MDB_FIRE_FP64 2
 
 /* MDConfig{} value-initialised defaults (include/md_config.hpp:14-75). */
 int mdb_config_default(mdb_config_t* out);

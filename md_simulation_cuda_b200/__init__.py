@@ -26,7 +26,8 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import (MDB_ERR_ARG, MDBConfigC, MDBError, MDBFireParams, MDBMinimizeResult,
+from ._lib import (FIRE_AUTO, FIRE_FP32, FIRE_FP64, MDB_ERR_ARG, MDBConfigC, MDBError,
+                   MDBFireParams, MDBMinimizeResult,
                    MDBNphProtocol, MDBNphRecord, MDBNphResult, MDBObservables, MDBRequest,
                    MDBRequestResult, MDBServerOptions, MDBServerStats, PARTICLE_DTYPE, check,
                    frame_ptr, lib, options)
@@ -380,13 +381,14 @@ class EnergyMinimizer:
     """EnergyMinimizer (include/md_energy_minimizer.hpp:37-97)."""
 
     def __init__(self, config_manager, comm=None, *, device: int = 0,
-                 skin: Optional[float] = None, use_graphs: bool = True):
+                 skin: Optional[float] = None, use_graphs: bool = True,
+                 fire_precision: Optional[int] = None):
         self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
             else MDConfigManager(_config_of(config_manager))
         # allocate_buffers (src/md_energy_minimizer.cu:92-100)
         if self.cfg_manager.config.n_cap <= 0:
             raise RuntimeError("EnergyMinimizer: n_cap must be positive.")
-        self._opt = options(device, skin, use_graphs)
+        self._opt = options(device, skin, use_graphs, fire_precision=fire_precision)
 
     def minimize_frame(self, frame, force_tol: float, max_steps: int,
                        params: FireParams) -> MinimizeResult:
@@ -514,9 +516,10 @@ class Batch:
     """Many independent systems advanced together on one GPU: FIRE quenches
     (add_fire) or MD segments of one kind (add_md)."""
 
-    def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True):
+    def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True,
+                 fire_precision: Optional[int] = None):
         self._h = C.c_void_p()
-        self._opt = options(device, skin, use_graphs)
+        self._opt = options(device, skin, use_graphs, fire_precision=fire_precision)
         check(lib().mdb_batch_create(C.byref(self._opt), C.byref(self._h)))
         self._sizes = []
         self._caps = []

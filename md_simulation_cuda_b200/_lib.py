@@ -100,7 +100,8 @@ class MDBOptions(C.Structure):
         ("use_graphs", C.c_int32),
         ("max_neighbors", C.c_int32),
         ("stream_priority", C.c_int32),
-        ("reserved", C.c_int32 * 11),
+        ("fire_precision", C.c_int32),
+        ("reserved", C.c_int32 * 10),
     ]
 
 
@@ -360,10 +361,16 @@ def check(rc: int):
     return rc
 
 
-def options(device=0, skin=None, use_graphs=True, max_neighbors=None) -> MDBOptions:
+FIRE_AUTO, FIRE_FP32, FIRE_FP64 = 0, 1, 2
+
+
+def options(device=0, skin=None, use_graphs=True, max_neighbors=None,
+            fire_precision=None) -> MDBOptions:
     o = MDBOptions()
     lib().mdb_options_default(C.byref(o))
     o.device = device
+    if fire_precision is not None:
+        o.fire_precision = int(fire_precision)
     if skin is not None:
         o.skin = float(skin)
     o.use_graphs = 1 if use_graphs else 0

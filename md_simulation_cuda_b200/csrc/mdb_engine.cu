@@ -51,6 +51,7 @@ Engine::Engine(const mdb_options_t& opt) {
   use_graphs_ = opt.use_graphs != 0;
   max_nbr_ = opt.max_neighbors > 0 ? opt.max_neighbors : (opt.max_neighbors < 0 ? 0 : 48);
   stream_priority_ = opt.stream_priority > 0 ? opt.stream_priority : 0;
+  fire_prec_ = opt.fire_precision;
   // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
   // see kernel nodes of graphs that contain conditional nodes).
   const char* eager = getenv("MDB_EAGER");
@@ -217,6 +218,11 @@ int Engine::build() {
     P.f_Nmin = sp.fire.N_min;
     P.f_tol = sp.tol;
     P.f_max_steps = sp.max_steps;
+    // FIRE pair arithmetic: FP32 pair terms leave a noise floor near 1e-6 in
+    // max |a|, so the automatic mode switches a system to FP64 pair terms
+    // once its max |a| is below 1e-3 (the switch is sticky).
+    P.f_hp_below = fire_prec_ == MDB_FIRE_FP32 ? -1.0
+                   : fire_prec_ == MDB_FIRE_FP64 ? HUGE_VAL : kFireFp64Below;
     P.target_steps = sp.target_steps;
     SysState& S = hst[s];
     memset(&S, 0, sizeof(S));
@@ -231,6 +237,7 @@ int Engine::build() {
     S.allpairs = 1;
     S.f_dt = sp.fire.dt_init;
     S.f_alpha = sp.fire.alpha0;
+    S.f_fp64 = (sp.kind == K_FIRE && fire_prec_ == MDB_FIRE_FP64) ? 1 : 0;
     p0 += n;
     b0 += P.nb;
     c0 += (int64_t)P.ccap_x * P.ccap_y;

@@ -113,6 +113,7 @@ class Engine {
   int rb_grid_ = 0;
   int scan_grid_ = 0;
   int nlist_grid_ = 0;
+  int fire_prec_ = MDB_FIRE_AUTO;
   int stream_priority_ = 0;  // levels above normal for stream_  // k_rb_nlist: one wave of resident blocks
   int64_t aos_cap_ = 0;
   void* d_aos_ = nullptr;

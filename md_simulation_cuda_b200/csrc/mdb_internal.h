@@ -24,6 +24,7 @@ namespace mdb {
 constexpr int kThreads = 256;  // particle kernels: one particle per thread
 constexpr double kSkinMD = 0.45;   // automatic list skin: MD systems
 constexpr double kSkinFire = 0.2;  // automatic list skin: a handle of FIRE systems only
+constexpr double kFireFp64Below = 1e-3;  // FIRE: FP64 pair terms below this max |a|
 constexpr int kNP = 6;         // reduction slots per block
 constexpr int kScanItems = 4;  // cells per thread in the scan kernels
 constexpr int kScanBlock = 512;
@@ -65,6 +66,7 @@ struct SysParams {
   float fsig2[3], feps24[3], feps4[3], frc2[3];
   // FIRE
   double f_dt_max, f_alpha0, f_inc, f_dec, f_tol;
+  double f_hp_below;  // FP64 pair terms once max |a| < f_hp_below (< 0: never)
   int32_t f_Nmin, f_max_steps;
   int64_t target_steps;  // MD segment length (batches)
 };
@@ -94,6 +96,8 @@ struct SysState {
   int32_t f_streak, f_conv, f_zero_v, f_step;
   int32_t f_conv_step;
   int32_t f_drift;  // the force phase of this iteration ran and did not converge
+  int32_t f_fp64;   // FP64 pair terms for this system (FIRE and its observations)
+  int32_t f_pad;
 };
 
 struct BatchGlobal {

@@ -183,7 +183,8 @@ __device__ __forceinline__ bool reduce_system(const Dev& D, const SysParams& P, 
 struct ForceTail {
   int64_t steps, target_steps;
   double pA, p_ext, fl, ce, vp, W, f_dt, f_alpha, f_tol, f_inc, f_dt_max, f_dec, f_alpha0;
-  int clamped, f_streak, f_step, f_Nmin;
+  double f_hp_below;
+  int clamped, f_streak, f_step, f_Nmin, f_fp64;
 };
 template <int FM>
 __device__ __forceinline__ ForceTail force_tail_inputs(const SysParams& P, const SysState* S) {
@@ -200,6 +201,8 @@ __device__ __forceinline__ ForceTail force_tail_inputs(const SysParams& P, const
     t.W = P.W;
   }
   if (FM == FM_FIRE) {
+    t.f_hp_below = P.f_hp_below;
+    t.f_fp64 = S->f_fp64;
     t.f_dt = S->f_dt;
     t.f_alpha = S->f_alpha;
     t.f_streak = S->f_streak;
@@ -294,6 +297,7 @@ struct PairCtx {
   float Lxh, Lxl, invLx, Lyh, Lyl, invLy;
   uint32_t ts;  // class whose pairs with i use the "same" parameters
   float rc2s, rc2ab, sig2s, sig2ab, e24s, e24ab, e4s, e4ab;
+  float r2fs, r2fab;  // FLOOR: smallest r^2 used in the pair term (1e-5 sigma_ij^2)
   double Vcs, Vcab;
 };
 
@@ -328,17 +332,21 @@ __device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float
 // candidate j: strict cutoff 0 < r^2 < rc_ij^2 in FP32, FP32 pair force, Kahan
 // FP32 accumulation. ENERGY adds 1/2 (u_ij - V_c) in FP64 (:795-807); VIRIAL
 // adds 1/2 r.F (:676-686) as the compensated FP32 sum of tmp*r^2.
-template <bool PY, bool ENERGY, bool VIRIAL, bool MIC = true>
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC = true, bool FLOOR = false>
 __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float& fxs, float& fxc,
                                          float& fys, float& fyc, float& ws, float& wc,
                                          double& u, double& an) {
   float dx, dy;
-  const float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
+  float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
   const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
   const bool same = (tj == c.ts);
   const float rc2 = same ? c.rc2s : c.rc2ab;
   // 0 < r2 < rc2 for the non-negative r2 (NaN fails): bits - 1 as unsigned
   if (__float_as_uint(r2) - 1u < __float_as_uint(rc2) - 1u) {
+    // FLOOR (FIRE and observations): pairs closer than ~0.003 sigma (random
+    // starts) take the pair term at r^2 = 1e-5 sigma^2, which keeps it finite
+    // in FP32; the reference's FP32 term overflows to inf/NaN there.
+    if (FLOOR) r2 = fmaxf(r2, same ? c.r2fs : c.r2fab);
     const float sig2 = same ? c.sig2s : c.sig2ab;
     const float e24 = same ? c.e24s : c.e24ab;
     const float r2i = recip(r2);
@@ -367,7 +375,7 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
 // else int32 at nlist[k * ntot + i]. MIC = false is the interior form: no
 // minimum image and no offset wrap (j = i + d). Offsets are fetched several at
 // a time before the dependent position gathers to keep loads in flight.
-template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, typename IDX>
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, bool FLOOR, typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
                                           int li, int n, int nn, const PairCtx& c, float& fxs,
@@ -392,7 +400,8 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
     }
 #pragma unroll
     for (int q = 0; q < PF; ++q)
-      pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc, u, an);
+      pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc,
+                                               u, an);
   }
   for (; k < nn; ++k) {
     int t = (int)__ldg(p + (int64_t)k * ntot);
@@ -401,18 +410,19 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
       t += (t < 0) ? n : 0;
       t -= (t >= n) ? n : 0;
     }
-    pair_one<PY, ENERGY, VIRIAL, MIC>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u, an);
+    pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u, an);
   }
 }
 
 // Candidates j in [j0, j1) (cell stencil rows or the whole system).
-template <bool PY, bool ENERGY, bool VIRIAL>
+template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR>
 __device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
                                            const PairCtx& c, float& fxs, float& fxc, float& fys,
                                            float& fyc, float& ws, float& wc, double& u,
                                            double& an) {
 #pragma unroll 4
-  for (int j = j0; j < j1; ++j) pair_one<PY, ENERGY, VIRIAL>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u, an);
+  for (int j = j0; j < j1; ++j)
+    pair_one<PY, ENERGY, VIRIAL, true, FLOOR>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u, an);
 }
 
 __device__ __forceinline__ void split_box(double L, float& h, float& l, float& inv) {
@@ -438,7 +448,7 @@ __device__ __forceinline__ void set_profile_class(PairCtx& c, const SysParams& P
 // system for grids narrower than 3 cells). Returns F in FP64. tci receives the
 // type class of slot i, decoded from the sign bits of its float-float
 // position (encode_ff), so the type array is not read.
-template <bool PY, bool ENERGY, bool VIRIAL>
+template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR = false>
 __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
                                                int64_t i, double Lx, double Ly, double& fx,
                                                double& fy, double& w, double& u, double& an,
@@ -464,6 +474,10 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   c.e4ab = P.feps4[2];
   c.Vcs = P.Vc[sc];
   c.Vcab = P.Vc[2];
+  if (FLOOR) {
+    c.r2fs = 1e-5f * P.fsig2[sc];
+    c.r2fab = 1e-5f * P.fsig2[2];
+  }
   float fxs = 0.f, fxc = 0.f, fys = 0.f, fyc = 0.f, ws = 0.f, wc = 0.f;
   u = 0.0;
   an = 0.0;
@@ -474,21 +488,21 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
     const int nn = nc & (kListInterior - 1);
     if (D.nl16) {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                              fys, fyc, ws, wc, u, an);
       else
-        pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                             fys, fyc, ws, wc, u, an);
     } else {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                              fys, fyc, ws, wc, u, an);
       else
-        pair_list<PY, ENERGY, VIRIAL, true>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
                                             fys, fyc, ws, wc, u, an);
     }
   } else if (S.allpairs) {
-    pair_range<PY, ENERGY, VIRIAL>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
+    pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
                                    wc, u, an);
   } else {
     const int ncx = S.ncx, ncy = S.ncy;
@@ -506,17 +520,17 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
       }
       const int64_t row = P.c0 + (int64_t)yy * ncx;
       if (cx > 0 && cx < ncx - 1) {
-        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + cx - 1), __ldg(cs + row + cx + 2), c,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + cx - 1), __ldg(cs + row + cx + 2), c,
                                        fxs, fxc, fys, fyc, ws, wc, u, an);
       } else if (cx == 0) {
-        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fxs, fxc, fys,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fxs, fxc, fys,
                                        fyc, ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 1), __ldg(cs + row + ncx), c,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 1), __ldg(cs + row + ncx), c,
                                        fxs, fxc, fys, fyc, ws, wc, u, an);
       } else {
-        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 2), __ldg(cs + row + ncx), c,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 2), __ldg(cs + row + ncx), c,
                                        fxs, fxc, fys, fyc, ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fxs, fxc,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fxs, fxc,
                                        fys, fyc, ws, wc, u, an);
       }
     }
@@ -524,6 +538,163 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   fx = (double)fxs - (double)fxc;
   fy = (double)fys - (double)fyc;
   w = 0.5 * ((double)ws - (double)wc);
+}
+
+// ------------------------------------------------- FP64 pair terms (FIRE) --
+// The same candidates as particle_force with every pair term in FP64: the
+// float-float coordinates converted to double are exact (hi and lo together
+// hold 48 bits), their difference is exact, the nearest image and the LJ
+// term are FP64 and the sums are FP64. Used by FIRE systems near convergence,
+// where FP32 pair terms leave a force noise floor near 1e-6.
+struct PairCtxD {
+  double xi, yi, Lx, Ly, invLx, invLy;
+  uint32_t ts;
+  double rc2s, rc2ab, sig2s, sig2ab, e24s, e24ab, e4s, e4ab, Vcs, Vcab;
+};
+
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC>
+__device__ __forceinline__ void pair_one_hp(const float4 q, const PairCtxD& c, double& fx,
+                                            double& fy, double& w, double& u, double& an) {
+  double dx = c.xi - ((double)fabsf(q.x) + (double)q.z);
+  double dy = c.yi - ((double)fabsf(q.y) + (double)q.w);
+  if (MIC) {
+    dx = fma(-rint(dx * c.invLx), c.Lx, dx);
+    if (PY) dy = fma(-rint(dy * c.invLy), c.Ly, dy);
+  }
+  const double r2 = fma(dx, dx, dy * dy);
+  const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
+  const bool same = (tj == c.ts);
+  const double rc2 = same ? c.rc2s : c.rc2ab;
+  if (r2 > 0.0 && r2 < rc2) {
+    const double sig2 = same ? c.sig2s : c.sig2ab;
+    const double r2e = fmax(r2, 1e-5 * sig2);  // the FP32 path's distance floor
+    const double r2i = 1.0 / r2e;
+    const double sr2 = sig2 * r2i;
+    const double sr6 = sr2 * sr2 * sr2;
+    const double sr12 = sr6 * sr6;
+    const double tmp = (same ? c.e24s : c.e24ab) * fma(2.0, sr12, -sr6) * r2i;
+    fx = fma(tmp, dx, fx);
+    fy = fma(tmp, dy, fy);
+    if (VIRIAL) w = fma(tmp, r2e, w);
+    if (ENERGY) {
+      u = fma(0.5, (same ? c.e4s : c.e4ab) * (sr12 - sr6) - (same ? c.Vcs : c.Vcab), u);
+      an += (tmp * dx) * dx - (tmp * dy) * dy;
+    }
+  }
+}
+
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, typename IDX>
+__device__ __forceinline__ void pair_list_hp(const float4* __restrict__ pff,
+                                             const IDX* __restrict__ nlist, int64_t ntot,
+                                             int64_t i, int li, int n, int nn, const PairCtxD& c,
+                                             double& fx, double& fy, double& w, double& u,
+                                             double& an) {
+  const float4* __restrict__ base = MIC ? pff + (i - li) : pff + i;
+  for (int k = 0; k < nn; ++k) {
+    int t = (int)__ldg(nlist + i + (int64_t)k * ntot);
+    if (MIC) {
+      t += li;
+      t += (t < 0) ? n : 0;
+      t -= (t >= n) ? n : 0;
+    }
+    pair_one_hp<PY, ENERGY, VIRIAL, MIC>(__ldg(base + t), c, fx, fy, w, u, an);
+  }
+}
+
+template <bool PY, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void pair_range_hp(const float4* __restrict__ pff, int j0, int j1,
+                                              const PairCtxD& c, double& fx, double& fy,
+                                              double& w, double& u, double& an) {
+  for (int j = j0; j < j1; ++j)
+    pair_one_hp<PY, ENERGY, VIRIAL, true>(__ldg(pff + j), c, fx, fy, w, u, an);
+}
+
+// FP64 counterpart of particle_force (same outputs; w already halved).
+template <bool PY, bool ENERGY, bool VIRIAL>
+__device__ __forceinline__ void particle_force_hp(const Dev& D, const SysParams& P,
+                                               const SysState& S, int64_t i, double Lx,
+                                               double Ly, double& fx, double& fy, double& w,
+                                               double& u, double& an) {
+  PairCtxD c;
+  const float4 qi = __ldg(D.pff + i);
+  c.xi = (double)fabsf(qi.x) + (double)qi.z;
+  c.yi = (double)fabsf(qi.y) + (double)qi.w;
+  c.Lx = Lx;
+  c.Ly = Ly;
+  c.invLx = 1.0 / Lx;
+  c.invLy = 1.0 / Ly;
+  const int tci = (int)((__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u));
+  c.ts = (tci == 2) ? 99u : (uint32_t)tci;
+  const int sc = (tci == 2) ? 2 : tci;
+  const double rs = P.cutoff * P.sig[sc], rab = P.cutoff * P.sig[2];
+  c.rc2s = rs * rs;
+  c.rc2ab = rab * rab;
+  c.sig2s = P.sig[sc] * P.sig[sc];
+  c.sig2ab = P.sig[2] * P.sig[2];
+  c.e24s = 24.0 * P.eps[sc];
+  c.e24ab = 24.0 * P.eps[2];
+  c.e4s = 4.0 * P.eps[sc];
+  c.e4ab = 4.0 * P.eps[2];
+  c.Vcs = P.Vc[sc];
+  c.Vcab = P.Vc[2];
+  fx = fy = w = u = an = 0.0;
+  const float4* __restrict__ pff = D.pff;
+  const int nc = __ldg(D.ncount + i);
+  if (nc >= 0) {
+    const int li = (int)(i - P.p0);
+    const int nn = nc & (kListInterior - 1);
+    const bool interior = (nc & kListInterior) != 0;
+    if (D.nl16) {
+      if (interior)
+        pair_list_hp<PY, ENERGY, VIRIAL, false>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fx,
+                                                fy, w, u, an);
+      else
+        pair_list_hp<PY, ENERGY, VIRIAL, true>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fx, fy,
+                                               w, u, an);
+    } else {
+      if (interior)
+        pair_list_hp<PY, ENERGY, VIRIAL, false>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fx, fy,
+                                                w, u, an);
+      else
+        pair_list_hp<PY, ENERGY, VIRIAL, true>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fx, fy,
+                                               w, u, an);
+    }
+  } else if (S.allpairs) {
+    for (int64_t j = P.p0; j < P.p0 + P.n; ++j) {
+      if (j == i) continue;
+      pair_one_hp<PY, ENERGY, VIRIAL, true>(__ldg(pff + j), c, fx, fy, w, u, an);
+    }
+  } else {
+    const int ncx = S.ncx, ncy = S.ncy;
+    const int cell = D.cell_of[i];
+    const int cx = cell % ncx, cy = cell / ncx;
+    const int* __restrict__ cs = D.cstart;
+    for (int dr = -1; dr <= 1; ++dr) {
+      int yy = cy + dr;
+      if (PY) {
+        if (yy < 0) yy += ncy;
+        if (yy >= ncy) yy -= ncy;
+      } else if (yy < 0 || yy >= ncy) {
+        continue;
+      }
+      const int64_t row = P.c0 + (int64_t)yy * ncx;
+      if (cx > 0 && cx < ncx - 1) {
+        pair_range_hp<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + cx - 1), __ldg(cs + row + cx + 2),
+                                          c, fx, fy, w, u, an);
+      } else if (cx == 0) {
+        pair_range_hp<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fx, fy, w,
+                                          u, an);
+        pair_range_hp<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 1), __ldg(cs + row + ncx),
+                                          c, fx, fy, w, u, an);
+      } else {
+        pair_range_hp<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row + ncx - 2), __ldg(cs + row + ncx),
+                                          c, fx, fy, w, u, an);
+        pair_range_hp<PY, ENERGY, VIRIAL>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fx, fy, w,
+                                          u, an);
+      }
+    }
+  }
+  w = 0.5 * w;
 }
 
 // Soft walls of piston_wall_kernel (src/md_cuda_common.cu:498-552) for one
@@ -550,59 +721,23 @@ __device__ __forceinline__ double wall_terms(double y, double Ly, double k, doub
   return wf;
 }
 
-// ------------------------------------------------------------ force phase --
-// One thread per slot. FM selects what follows the force evaluation; PY is the
-// y image convention (false = the piston's walled y axis, which also applies
-// the soft walls in FM_INIT/FM_OBS).
+// What follows the pair sum of one slot in the force phase: the kick, the
+// reductions and the stores (the sums are the caller's per-thread partials).
 template <int FM, bool PY>
-__global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
-  const int b = blockIdx.x;
-  const int s = D.sys_of_block[b];
-  const SysParams& P = D.sp[s];
-  SysState* S = D.st + s;
-  {
-    // L1 prefetch of this thread's first slot and its first list rows
-    const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
-    if (i0 < P.p0 + P.n) {
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.pff + i0));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.vel + i0));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.ncount + i0));
-      if (D.nl16 && D.max_nbr >= 8) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          asm volatile("prefetch.global.L1 [%0];" ::"l"(D.nlist16 + (int64_t)q * D.ntot + i0));
-      }
-    }
-  }
-  // a finished batch system is still observed (FM_OBS) and re-evaluated (FM_INIT)
-  const bool skip = (FM != FM_OBS && FM != FM_INIT && S->done != 0) || (S->err != 0) ||
-                    (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
-  constexpr bool kEnergy = (FM == FM_OBS);
-  constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
-  constexpr int kNS = ForceRed<FM>::NS, kNM = ForceRed<FM>::NM;
+struct ForceFinish {
   double red[kNP];
+  double mx[3];
+  int bad;
+  __device__ __forceinline__ void init() {
 #pragma unroll
-  for (int k = 0; k < kNP; ++k) red[k] = 0.0;
-  double mx[3] = {0.0, 0.0, 0.0};
-  int bad = 0;
-  const double Lx = S->Lx, Ly = S->Ly;
-  const double dt = P.dt, h = 0.5 * dt;
-  const int items = P.items;
-  // Block b of the system takes the kThreads-slot chunks b, b + nb, b + 2 nb,
-  // ...: the chunks of one block come from across the whole system, so dense
-  // and sparse regions (different list lengths) even out between blocks.
-  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
-  const int64_t stride = (int64_t)P.nb * kThreads;
-  const int64_t end = P.p0 + P.n;
-  const double xi2 = (FM == FM_NH) ? S->xi : 0.0;
-  const double fdt = (FM == FM_FIRE) ? S->f_dt : 0.0;
-#pragma unroll 1
-  for (int it = 0; it < items; ++it) {
-    const int64_t i = base + (int64_t)it * stride;
-    if (skip || i >= end) break;
-    double fx, fy, w, u, an;
-    int tci;
-    particle_force<PY, kEnergy, kVirial>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an, tci);
+    for (int k = 0; k < kNP; ++k) red[k] = 0.0;
+    mx[0] = mx[1] = mx[2] = 0.0;
+    bad = 0;
+  }
+  __device__ __forceinline__ void operator()(const Dev& D, const SysParams& P, double Ly,
+                                             double h, double xi2, double fdt, int64_t i,
+                                             double fx, double fy, double w, double u, double an,
+                                             int tci) {
     const double m = (tci == 0) ? P.massA : P.massB;  // type 0 <=> class 0
     double2 v = D.vel[i];
     if (FM == FM_OBS) {
@@ -663,12 +798,99 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       if (!isfinite(ax) || !isfinite(ay) || !isfinite(v.x) || !isfinite(v.y)) bad = 1;
     }
   }
-  if (bad) atomicOr(&S->nonfinite, 1);
+};
+
+// The force phase's slots of one thread with FP64 pair terms (a FIRE system
+// past its switch point, and its observations). Out of line: its registers
+// do not count against the FP32 pair loop of the kernel.
+template <int FM, bool PY>
+__device__ __noinline__ ForceFinish<FM, PY> force_items_hp(Dev D, const SysParams* Pp,
+                                                           const SysState* Sp, int64_t base,
+                                                           int64_t stride, int64_t end,
+                                                           int items, double Lx, double Ly,
+                                                           double h, double xi2, double fdt) {
+  constexpr bool kEnergy = (FM == FM_OBS);
+  constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
+  const SysParams& P = *Pp;
+  ForceFinish<FM, PY> fin;
+  fin.init();
+  for (int it = 0; it < items; ++it) {
+    const int64_t i = base + (int64_t)it * stride;
+    if (i >= end) break;
+    double fx, fy, w, u, an;
+    const float4 qi = __ldg(D.pff + i);
+    const int tci = (int)((__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u));
+    particle_force_hp<PY, kEnergy, kVirial>(D, P, *Sp, i, Lx, Ly, fx, fy, w, u, an);
+    fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
+  }
+  return fin;
+}
+
+// ------------------------------------------------------------ force phase --
+// One thread per slot. FM selects what follows the force evaluation; PY is the
+// y image convention (false = the piston's walled y axis, which also applies
+// the soft walls in FM_INIT/FM_OBS).
+template <int FM, bool PY>
+__global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
+  const int b = blockIdx.x;
+  const int s = D.sys_of_block[b];
+  const SysParams& P = D.sp[s];
+  SysState* S = D.st + s;
+  {
+    // L1 prefetch of this thread's first slot and its first list rows
+    const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+    if (i0 < P.p0 + P.n) {
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.pff + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.vel + i0));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(D.ncount + i0));
+      if (D.nl16 && D.max_nbr >= 8) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(D.nlist16 + (int64_t)q * D.ntot + i0));
+      }
+    }
+  }
+  // a finished batch system is still observed (FM_OBS) and re-evaluated (FM_INIT)
+  const bool skip = (FM != FM_OBS && FM != FM_INIT && S->done != 0) || (S->err != 0) ||
+                    (FM == FM_FIRE && (S->f_conv != 0 || S->f_step >= P.f_max_steps));
+  constexpr bool kEnergy = (FM == FM_OBS);
+  constexpr bool kVirial = (FM == FM_OBS || FM == FM_NPH);
+  constexpr int kNS = ForceRed<FM>::NS, kNM = ForceRed<FM>::NM;
+  const double Lx = S->Lx, Ly = S->Ly;
+  const double dt = P.dt, h = 0.5 * dt;
+  const int items = P.items;
+  // Block b of the system takes the kThreads-slot chunks b, b + nb, b + 2 nb,
+  // ...: the chunks of one block come from across the whole system, so dense
+  // and sparse regions (different list lengths) even out between blocks.
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
+  const int64_t stride = (int64_t)P.nb * kThreads;
+  const int64_t end = P.p0 + P.n;
+  const double xi2 = (FM == FM_NH) ? S->xi : 0.0;
+  const double fdt = (FM == FM_FIRE) ? S->f_dt : 0.0;
+  // What follows the pair sum of one slot (kick, reductions, stores).
+  constexpr bool kHpCapable = (FM == FM_FIRE || FM == FM_OBS || FM == FM_INIT);
+  ForceFinish<FM, PY> fin;
+  if (kHpCapable && !skip && S->f_fp64 != 0) {
+    fin = force_items_hp<FM, PY>(D, &P, S, base, stride, end, items, Lx, Ly, h, xi2, fdt);
+  } else {
+    fin.init();
+#pragma unroll 1
+    for (int it = 0; it < items; ++it) {
+      const int64_t i = base + (int64_t)it * stride;
+      if (skip || i >= end) break;
+      double fx, fy, w, u, an;
+      int tci;
+      particle_force<PY, kEnergy, kVirial, kHpCapable>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an,
+                                                       tci);
+      fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
+    }
+  }
+  if (fin.bad) atomicOr(&S->nonfinite, 1);
   ForceTail tin;
   if (threadIdx.x == 0) tin = force_tail_inputs<FM>(P, S);
   double tot[kNP];
   double tmx[3];
-  if (!reduce_system<kNS, kNM>(D, P, S, red, mx, tot, tmx)) return;
+  if (!reduce_system<kNS, kNM>(D, P, S, fin.red, fin.mx, tot, tmx)) return;
   if (threadIdx.x != 0) return;
   int conv = 0;
   if (!skip) {
@@ -715,6 +937,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       const double maxf = (tmx[1] > 0.0) ? __longlong_as_double(0x7ff8000000000000ULL) : tmx[0];
       S->f_power = tot[0];
       S->f_maxf = maxf;
+      // from the next iteration on, FP64 pair terms for this system
+      if (!tin.f_fp64 && maxf < tin.f_hp_below) S->f_fp64 = 1;
       if (maxf < tin.f_tol) {
         conv = 1;
         S->f_conv = 1;
