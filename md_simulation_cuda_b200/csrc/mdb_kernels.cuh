@@ -1012,8 +1012,8 @@ __device__ __forceinline__ void drift_particle(const Dev& D, const DriftCtx& c, 
     v.y = fma(c.h, a.y, v.y);
     v.x = v.x * c.vsc;
     v.y = v.y * c.vsc;
-    x.x = fma(c.dt, v.x, c.lam * x.x);
-    x.y = fma(c.dt, v.y, c.lam * x.y);
+    x.x = fma(c.lam, x.x, c.dt * v.x);
+    x.y = fma(c.lam, x.y, c.dt * v.y);
   } else if (DMd == DM_FIRE) {
     // zero_velocity / fire_velocity_mix / drift (src/md_energy_minimizer.cu:32-71)
     if (c.zero_v) {

@@ -103,7 +103,9 @@ static inline void pair_mixed(const or_lj_t* lj, double xi, double yi, int ti, d
     const float fy_f = tmp_f * dy_f;
     a->fx += (double)fx_f;
     a->fy += (double)fy_f;
-    const float u_pair_f = (4.0f * epsilon_f) * (sr12_f - sr6_f);
+    /* the reference's build contracts sr6*sr6 - sr6 into one fused
+     * multiply-add in cal_local_U_kernel (pinned against its outputs) */
+    const float u_pair_f = (4.0f * epsilon_f) * fmaf(sr6_f, sr6_f, -sr6_f);
     a->u = fma(0.5, (double)u_pair_f - shift_of(lj, c), a->u);
     a->w = fma(0.5, fma((double)dx_f, (double)fx_f, (double)dy_f * (double)fy_f), a->w);
   }
@@ -266,7 +268,7 @@ static inline ref_pair_t ref_pair_terms(const or_lj_t* lj, int mode, double xi, 
   r.dy = (double)dy_f;
   r.fx = (double)(tmp_f * dx_f);
   r.fy = (double)(tmp_f * dy_f);
-  r.u = (double)((4.0f * epsilon_f) * (sr12_f - sr6_f));
+  r.u = (double)((4.0f * epsilon_f) * fmaf(sr6_f, sr6_f, -sr6_f));
   return r;
 }
 
@@ -761,8 +763,21 @@ void or_sim_setup(or_sim_t* s) {
   or_sim_cal_forces(s, 1);
 }
 
+/* Sum of the reference kernel `what` over the system through its block
+ * trees (ref_threads per block) and the host's block-order loop. */
+static double ref_tree_total(const or_sim_t* s, int what, int32_t periodic_y) {
+  double* v = (double*)malloc(sizeof(double) * (size_t)(s->n + 1));
+  if (!v) return NAN;
+  or_ref_thread_values(&s->lj, s->n, s->pos, s->vel, s->type, s->Lx, s->Ly, periodic_y, s->mode,
+                       s->ws1_halo, what, 0.0, v, s->nthreads);
+  const double tot = or_ref_block_partials(s->n, v, s->ref_threads, NULL);
+  free(v);
+  return tot;
+}
+
 /* cal_local_K_kernel (src/md_cuda_common.cu:554-589): k = 1/2 m |v|^2. */
 double or_total_K(const or_sim_t* s) {
+  if (s->ref_threads > 0) return ref_tree_total(s, OR_SUM_K, 1);
   double K = 0.0;
   for (int64_t i = 0; i < s->n; ++i) {
     const double vx = s->vel[2 * i], vy = s->vel[2 * i + 1];
@@ -776,6 +791,10 @@ double or_total_K(const or_sim_t* s) {
  * (sum m|v|^2 + sum_i 1/2 sum_j r.F) / (2 A). */
 double or_scalar_pressure(or_sim_t* s, int32_t periodic_y) {
   const double area = s->Lx * s->Ly;
+  if (s->ref_threads > 0) {
+    const double sum = ref_tree_total(s, OR_SUM_P, periodic_y);
+    return (area > 0.0) ? sum / (2.0 * area) : 0.0;
+  }
   double kin = 0.0;
   for (int64_t i = 0; i < s->n; ++i) {
     const double vx = s->vel[2 * i], vy = s->vel[2 * i + 1];
@@ -792,6 +811,9 @@ double or_scalar_pressure(or_sim_t* s, int32_t periodic_y) {
 static void piston_walls(or_sim_t* s, int update_acc, double* upper, double* energy) {
   double up = 0.0, en = 0.0;
   const double k = s->k_piston;
+  double* tv = NULL;
+  if (s->ref_threads > 0 && s->n > 0 && k > 0.0)
+    tv = (double*)malloc(sizeof(double) * (size_t)(2 * s->n));
   if (s->n > 0 && k > 0.0) {
     for (int64_t i = 0; i < s->n; ++i) {
       const double y = s->pos[2 * i + 1];
@@ -813,17 +835,33 @@ static void piston_walls(or_sim_t* s, int update_acc, double* upper, double* ene
       }
       up += upi;
       en += eni;
+      if (tv) {
+        tv[i] = upi;
+        tv[s->n + i] = eni;
+      }
     }
+  }
+  if (tv) {
+    up = or_ref_block_partials(s->n, tv, s->ref_threads, NULL);
+    en = or_ref_block_partials(s->n, tv + s->n, s->ref_threads, NULL);
+    free(tv);
   }
   *upper = up;
   *energy = en;
+}
+
+void or_sim_piston_walls(or_sim_t* s, int32_t update_acc, double* upper, double* energy) {
+  piston_walls(s, update_acc, upper, energy);
 }
 
 /* cal_total_U (src/md_env.cu:2347-2360). */
 double or_total_U(or_sim_t* s) {
   const int periodic_y = s->piston_mode_active ? 0 : 1;
   double U = 0.0;
-  sim_forces(s, periodic_y, NULL, &U, NULL);
+  if (s->ref_threads > 0)
+    U = ref_tree_total(s, OR_SUM_U, periodic_y);
+  else
+    sim_forces(s, periodic_y, NULL, &U, NULL);
   if (!s->piston_mode_active) return U;
   double up, en;
   piston_walls(s, 0, &up, &en);
@@ -960,7 +998,7 @@ void or_step_nph(or_sim_t* s, double p_ext) {
     for (int d = 0; d < 2; ++d) {
       const int64_t k = 2 * i + d;
       s->vel[k] = s->vel[k] * vs;
-      s->pos[k] = fma(dt, s->vel[k], lin * s->pos[k]);
+      s->pos[k] = fma(lin, s->pos[k], dt * s->vel[k]);
     }
     s->pos[2 * i] = or_pbc_wrap(s->pos[2 * i], Lx_new);
     s->pos[2 * i + 1] = or_pbc_wrap(s->pos[2 * i + 1], Ly_new);
@@ -1045,6 +1083,51 @@ void or_step_nph_piston(or_sim_t* s, double p_ext) {
   }
   s->last_instant_pressure = s->piston_force / Lx;
   s->t += dt;
+}
+
+/* The reference's integrator kernels one at a time (src/md_cuda_common.cu:
+ * 379-496), in the arithmetic its build performs (pinned against outputs of
+ * the kernels themselves, tests/golden/ref_physics.*). */
+int or_ref_integrator(int32_t which, int64_t n, double* pos, double* vel, const double* acc,
+                      double dt, double xi, double lin, double vsc, double Lx, double Ly) {
+  if (which < 0 || which > 6 || n < 0) return 1;
+  const double h = 0.5 * dt;
+  for (int64_t i = 0; i < n; ++i) {
+    for (int d = 0; d < 2; ++d) {
+      const int64_t k = 2 * i + d;
+      double v = vel[k];
+      switch (which) {
+        case 0: /* step_half_vv_kernel :381-394 */
+        case 6: /* step_half_vv_piston_kernel :396-409 */
+          v = fma(h, acc[k], v);
+          pos[k] = fma(dt, v, pos[k]);
+          break;
+        case 1: /* step_2nd_half_vv_kernel :443-452 */
+        case 4: /* step_half_nph_velocity_kernel :411-420 */
+          v = fma(h, acc[k], v);
+          break;
+        case 2: /* step_half_vv_nh_kernel :454-478 */
+          v = fma(h, fma(-xi, v, acc[k]), v);
+          pos[k] = fma(dt, v, pos[k]);
+          break;
+        case 3: /* step_2nd_half_vv_nh_kernel :480-496 */
+          v = fma(h, fma(-xi, v, acc[k]), v);
+          break;
+        case 5: /* step_nph_scale_and_drift_kernel :422-440 */
+          v = v * vsc;
+          pos[k] = fma(lin, pos[k], dt * v);
+          break;
+      }
+      vel[k] = v;
+    }
+    if (which == 0 || which == 2 || which == 5) {
+      pos[2 * i] = or_pbc_wrap(pos[2 * i], Lx);
+      pos[2 * i + 1] = or_pbc_wrap(pos[2 * i + 1], Ly);
+    } else if (which == 6) {
+      pos[2 * i] = or_pbc_wrap(pos[2 * i], Lx);
+    }
+  }
+  return 0;
 }
 
 /* ---- FIRE ------------------------------------------------------------------ */

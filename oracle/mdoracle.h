@@ -138,6 +138,9 @@ typedef struct or_sim {
   int32_t use_cells; /* cell list instead of all pairs */
   int32_t nthreads;
   int32_t error;     /* nonzero after an invalid box (reference: MPI_Abort) */
+  int32_t ref_threads; /* > 0: K, U, P and wall sums through the reference's
+                          block trees of this many threads, then block order
+                          (bit-exact with its kernels); 0: sequential sums */
 } or_sim_t;
 
 /* Buffers are caller-owned; or_sim_setup fills the derived fields and computes
@@ -152,6 +155,19 @@ double or_total_K(const or_sim_t* s);
 double or_total_U(or_sim_t* s);
 double or_instant_pressure(or_sim_t* s);
 double or_scalar_pressure(or_sim_t* s, int32_t periodic_y);
+/* piston_wall_kernel + evaluate_piston_wall_observables (src/md_cuda_common.cu:
+ * 498-552, src/md_env.cu:2148-2203): upper-wall force and wall energy, and
+ * with update_acc the wall force added to acc.y. */
+void or_sim_piston_walls(or_sim_t* s, int32_t update_acc, double* upper, double* energy);
+
+/* One of the reference's integrator kernels (src/md_cuda_common.cu:379-496)
+ * in place on n particles (pos, vel: 2n; acc: 2n read only):
+ * 0 step_half_vv (dt, Lx, Ly), 1 step_2nd_half_vv (dt),
+ * 2 step_half_vv_nh (dt, xi, Lx, Ly), 3 step_2nd_half_vv_nh (dt, xi),
+ * 4 step_half_nph_velocity (dt), 5 step_nph_scale_and_drift (dt, lin, vsc,
+ * Lx, Ly = the new box), 6 step_half_vv_piston (dt, Lx). */
+int or_ref_integrator(int32_t which, int64_t n, double* pos, double* vel, const double* acc,
+                      double dt, double xi, double lin, double vsc, double Lx, double Ly);
 
 /* ---- FIRE (EnergyMinimizer::minimize_frame) ----------------------------- */
 typedef struct or_fire_params {

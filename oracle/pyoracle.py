@@ -68,6 +68,7 @@ class OrSim(C.Structure):
         ("use_cells", C.c_int32),
         ("nthreads", C.c_int32),
         ("error", C.c_int32),
+        ("ref_threads", C.c_int32),
     ]
 
 
@@ -133,6 +134,9 @@ def lib():
                                                C.c_double, C.c_double, C.c_int32, C.c_int32,
                                                C.c_int32, C.c_int32, C.c_double, dp, C.c_int32]
             L.or_ref_block_partials.argtypes = [C.c_int64, dp, C.c_int32, dp]
+            L.or_ref_integrator.argtypes = [C.c_int32, C.c_int64, dp, dp, dp, C.c_double,
+                                            C.c_double, C.c_double, C.c_double, C.c_double,
+                                            C.c_double]
             L.or_ref_block_partials.restype = C.c_double
             L.or_cell_grid.argtypes = [C.c_double, C.c_double, C.c_double, ip, ip]
             L.or_cell_bin.argtypes = [C.c_int64, dp, C.c_double, C.c_double, C.c_int32,
@@ -144,6 +148,8 @@ def lib():
             for name in ("or_sim_setup", "or_step_nve", "or_step_nose_hoover"):
                 getattr(L, name).argtypes = [sp]
             L.or_sim_cal_forces.argtypes = [sp, C.c_int32]
+            L.or_sim_piston_walls.argtypes = [sp, C.c_int32, dp, dp]
+            L.or_sim_piston_walls.restype = None
             L.or_step_nph.argtypes = [sp, C.c_double]
             L.or_step_nph_piston.argtypes = [sp, C.c_double]
             for name in ("or_total_K", "or_total_U", "or_instant_pressure"):
@@ -298,6 +304,16 @@ def ref_block_partials(values, threads=256):
     return tot, part[:nb]
 
 
+def ref_integrator(which, pos, vel, acc, dt, xi=0.0, lin=1.0, vsc=1.0, Lx=0.0, Ly=0.0):
+    """One of the reference's integrator kernels (or_ref_integrator): new (pos, vel)."""
+    p = np.array(_pos2(pos), dtype=np.float64, copy=True)
+    v = np.array(_pos2(vel), dtype=np.float64, copy=True)
+    a = np.ascontiguousarray(_pos2(acc), dtype=np.float64)
+    assert lib().or_ref_integrator(which, p.shape[0], _dp(p), _dp(v), _dp(a), dt, xi, lin, vsc,
+                                   Lx, Ly) == 0
+    return p, v
+
+
 def cell_build(pos, Lx, Ly, cell_min):
     """Project binning: (cell ids, stable permutation, ncx, ncy)."""
     p = _pos2(pos)
@@ -321,7 +337,7 @@ class Sim:
     """Stateful oracle engine mirroring MDSimulation's hot path."""
 
     def __init__(self, cfg, pos, vel, types, mode=OR_FP64, ws1_halo=0, use_cells=True,
-                 nthreads=0):
+                 nthreads=0, ref_threads=0):
         self.pos = np.array(_pos2(pos), dtype=np.float64, copy=True)
         n = self.pos.shape[0]
         self.vel = np.array(np.asarray(vel, dtype=np.float64).reshape(n, 2), copy=True)
@@ -349,6 +365,7 @@ class Sim:
         s.ws1_halo = ws1_halo
         s.use_cells = 1 if use_cells else 0
         s.nthreads = nthreads
+        s.ref_threads = ref_threads
         self.s = s
         lib().or_sim_setup(C.byref(s))
 
@@ -367,6 +384,16 @@ class Sim:
     def step_nph_piston(self, p_ext, n=1):
         for _ in range(n):
             lib().or_step_nph_piston(C.byref(self.s), p_ext)
+
+    def cal_forces(self, periodic_y=1):
+        lib().or_sim_cal_forces(C.byref(self.s), periodic_y)
+
+    def piston_walls(self, update_acc=False):
+        """(upper-wall force, wall energy); update_acc adds the walls to acc."""
+        up, en = C.c_double(), C.c_double()
+        lib().or_sim_piston_walls(C.byref(self.s), 1 if update_acc else 0, C.byref(up),
+                                  C.byref(en))
+        return up.value, en.value
 
     def total_K(self):
         return lib().or_total_K(C.byref(self.s))

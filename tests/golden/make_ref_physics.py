@@ -137,7 +137,8 @@ def record_static(name, cfg, frame, periodic_y, arrays, meta, threads=(256,)):
     meta[name] = m
 
 
-def record_traj(name, cfg, frame, kind, nsteps, p_ext, arrays, meta, ws1=0):
+def record_traj(name, start, cfg, frame, kind, nsteps, p_ext, arrays, meta, ws1=0):
+    """nsteps of one step kind from the frame of static case `start`."""
     s = rk.RefSim(cfg, frame, ws1_halo=bool(ws1), threads=256, init_forces=True)
     K, U = s.step(kind, nsteps, p_ext=p_ext, trace=True)
     f = s.frame()
@@ -147,7 +148,7 @@ def record_traj(name, cfg, frame, kind, nsteps, p_ext, arrays, meta, ws1=0):
     arrays[f"{name}/final_vel"] = f["vel"].copy()
     arrays[f"{name}/final_acc"] = f["acc"].copy()
     meta[name] = {"kind": kind, "nsteps": nsteps, "p_ext": p_ext, "ws1_halo": ws1,
-                  "cfg": cfg, "state": s.state()}
+                  "cfg": cfg, "state": s.state(), "start": start}
     s.close()
 
 
@@ -207,11 +208,11 @@ def main():
         s.close()
 
     # trajectories
-    record_traj("nve_lat512", c_lat, f, rk.KIND_NVE, 40, 0.0, arrays, meta)
-    record_traj("nve_lat512_ws1", c_lat, f, rk.KIND_NVE, 10, 0.0, arrays, meta, ws1=1)
-    record_traj("nh_slab512", c_slab, fs, rk.KIND_NH, 40, 0.0, arrays, meta)
-    record_traj("nph_lat512", c_lat, f, rk.KIND_NPH, 20, 1.0, arrays, meta)
-    record_traj("piston512", c_pis, fp, rk.KIND_PISTON, 20, 0.5, arrays, meta)
+    record_traj("nve_lat512", "lat512", c_lat, f, rk.KIND_NVE, 40, 0.0, arrays, meta)
+    record_traj("nve_lat512_ws1", "lat512", c_lat, f, rk.KIND_NVE, 10, 0.0, arrays, meta, ws1=1)
+    record_traj("nh_slab512", "slab512", c_slab, fs, rk.KIND_NH, 40, 0.0, arrays, meta)
+    record_traj("nph_lat512", "lat512", c_lat, f, rk.KIND_NPH, 20, 1.0, arrays, meta)
+    record_traj("piston_traj512", "piston512", c_pis, fp, rk.KIND_PISTON, 20, 0.5, arrays, meta)
 
     os.makedirs(a.out, exist_ok=True)
     np.savez_compressed(os.path.join(a.out, "ref_physics.npz"), **arrays)
