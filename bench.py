@@ -14,8 +14,12 @@ collective on the data path; time is the max over ranks.
 --impl reference times the reference's algorithm for this path on the host
 cores: its O(N^2) all-pairs force loop (src/md_cuda_common.cu:151-264) in the
 reference's mixed precision, restated by the CPU oracle, on a bounded sample of
-rows per step (the reference's CUDA build needs MPI and RAFT and cannot be
-built here).
+rows per step (the reference has no CPU implementation of its own).
+
+The main line also carries `reference_gpu`: the reference's own CUDA kernels
+(src/md_cuda_common.cu compiled unmodified into oracle/_ref/libref_kernels.so,
+driven by its host step logic at MPI world size 1, self-halo included) timed
+on the same GPU for the same workload.
 """
 from __future__ import annotations
 
@@ -145,16 +149,48 @@ def make_workload(name, rank):
                           "90%/10% A stripes, T=0.7, Q=1.0, dt=0.002")
 
 
-def step_roofline(per_gpu_value, hbm_gbs, p_ord):
-    """The survey's whole-step roofline: particle-steps/s on one GPU against
-    min(HBM bandwidth / 97 B per particle-step, FP32 peak / (24 flops x
-    ordered pairs inside the cutoff per particle))."""
-    bw_bound = hbm_gbs * 1e9 / 97.0
+def step_roofline(per_gpu_value, hbm_gbs, p_ord, bytes_per_step=97.0):
+    """Whole-step roofline: particle-steps/s on one GPU against
+    min(HBM bandwidth / bytes per particle-step, FP32 peak / (24 flops x
+    ordered pairs inside the cutoff per particle)). 97 B is the survey's
+    algorithmic figure (FP64 pos/vel/force read and written, 1 B type); this
+    design moves 173 B (force phase 65 B + drift phase 108 B)."""
+    bw_bound = hbm_gbs * 1e9 / bytes_per_step
     fp_bound = FP32_NOMINAL_TFLOPS * 1e12 / (24.0 * p_ord) if p_ord else float("inf")
     bound = min(bw_bound, fp_bound)
     return {"achieved": per_gpu_value, "bound": bound, "unit": "particle-steps/s",
+            "bytes_per_particle_step": bytes_per_step,
             "limited_by": "hbm" if bw_bound <= fp_bound else "fp32",
             "frac": per_gpu_value / bound}
+
+
+def reference_gpu_leg(f, cfg, mode, steps):
+    """The reference's own single-GPU build on this GPU: its kernels from
+    src/md_cuda_common.cu (compiled unmodified for sm_100a) and its host step
+    logic at world size 1, including the self-halo it rebuilds every step.
+    Device time (CUDA events around its host-synchronous loop) after one
+    untimed step."""
+    try:
+        from oracle import refkernels as rk
+
+        if not rk.available():
+            return {"unavailable": "oracle/_ref/libref_kernels.so not built"}
+        kind = {"nh": rk.KIND_NH, "nph": rk.KIND_NPH, "nve": rk.KIND_NVE}[mode]
+        p_ext = 1.0 if mode == "nph" else 0.0
+        r = rk.RefSim(cfg, f, ws1_halo=True, threads=int(cfg.get("THREADS_PER_BLOCK", 256) or 256))
+        r.step(kind, 1, p_ext=p_ext)
+        ms = r.time_steps(kind, steps, p_ext=p_ext)
+        r.close()
+        n = len(f)
+        return {"value": n * steps / (ms * 1e-3), "unit": "particle-steps/s",
+                "ms_per_step": ms / steps, "steps": steps,
+                "build": "src/md_cuda_common.cu unmodified, nvcc -O3 for sm_100a "
+                         "(oracle/build_ref.py); host step logic of src/md_env.cu at world "
+                         "size 1 restated in oracle/ref_kernels.cu",
+                "how": "CUDA events on the default stream around the host-synchronous "
+                       "step loop, after 1 untimed step"}
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": f"reference kernels failed: {e}"}
 
 
 def cpu_cell_baseline(f, cfg, mode_name, budget_s=20.0):
@@ -217,7 +253,10 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
     b.run(-1 if to_completion else iters)
     t_batch = max_over_ranks(time.perf_counter() - t0, dist, dev)
     s1 = steps_of(b, ids)
-    work = float((sizes * (s1 - s0)).sum())
+    # non-finite systems (none are expected: FP32 pair terms are floored at
+    # r^2 = 1e-5 sigma^2) do not count as work
+    finite = np.array([not b.fire_result(i, with_frame=False).nonfinite for i in ids])
+    work = float((sizes * (s1 - s0) * finite).sum())
     if dist is not None:
         import torch
 
@@ -251,6 +290,7 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
                        f"{warm_iters + iters}"),
             "seconds": t_batch, "build_and_warmup_s": t_build,
             "finished_systems": done, "converged_systems": converged,
+            "nonfinite_systems": int((~finite).sum()),
             "plain_path": {"value": plain, "unit": "particle-iterations/s",
                            "sample": f"{len(pick)} systems (every {max(1, len(order) // plain_sample)}"
                                      f"th by N), each alone as a batch of one, same window"},
@@ -553,6 +593,18 @@ def run_ours(args):
     if rank == 0 and ws == 1 and args.workload == "nvt_slab":
         batched = measure_fire_mix(dev, 100, 2000)
 
+    # ---- the reference's own CUDA build on this GPU (rank 0, N = 1) ---------
+    reference_gpu = None
+    if rank == 0 and ws == 1:
+        del sim
+        sim = None
+        torch.cuda.empty_cache()
+        ref_steps = {"nh": 3, "nph": 1, "nve": 1000}[mode]
+        reference_gpu = reference_gpu_leg(f, cfg, mode, ref_steps)
+        if "value" in reference_gpu:
+            reference_gpu["ours_over_reference"] = value / reference_gpu["value"]
+            reference_gpu["ours_e2e_over_reference"] = e2e["value"] / reference_gpu["value"]
+
     if rank == 0:
         achieved = force_bytes / t_force / 1e9
         out = {
@@ -581,12 +633,14 @@ def run_ours(args):
                                   "pairs_per_particle": p_ord},
                          # whole step: per-GPU particle-steps/s over the step's bound,
                          # min(HBM peak / 97 B, FP32 peak / (24 flops x P_ord))
-                         "step": step_roofline(value / ws, hbm_peak, p_ord)},
+                         "step": step_roofline(value / ws, hbm_peak, p_ord),
+                         "step_design": step_roofline(value / ws, hbm_peak, p_ord, 173.0)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clk,
             "batched": batched,
+            "reference_gpu": reference_gpu,
         }
         print(json.dumps(out), flush=True)
     del sim
