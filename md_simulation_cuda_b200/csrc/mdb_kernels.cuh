@@ -45,22 +45,42 @@ __device__ __forceinline__ double type_mass(const SysParams& P, int t) {
   return t == 0 ? P.massA : P.massB;
 }
 
-// Exact float-float split of a biased coordinate. X = x + off lies in one
-// binade [B, 2B), so the difference of two hi parts is exact; lo carries the
-// next 24 bits. The sign bits of the hi parts carry the type class
-// (x: class 1, y: class 2).
+// Float-float split of a biased coordinate. X = x + off lies in one binade
+// [B, 2B), so the difference of two hi parts is exact; lo carries the next 24
+// bits. The lowest mantissa bit of each lo part carries one bit of the type
+// class (x: bit 0, y: bit 1), which moves the coordinate by at most 2^-47 B
+// (1.5e-11 for B = 4096); the hi parts stay positive, so the pair loop can
+// subtract x and y together with one packed FP32x2 instruction.
 __device__ __forceinline__ float4 encode_ff(double x, double y, int t, double offx, double offy) {
   const double X = x + offx;
   const double Y = y + offy;
-  float xh = __double2float_rn(X);
+  const float xh = __double2float_rn(X);
   const float xl = __double2float_rn(X - (double)xh);
-  float yh = __double2float_rn(Y);
+  const float yh = __double2float_rn(Y);
   const float yl = __double2float_rn(Y - (double)yh);
-  const int tc = type_class(t);
-  if (tc == 1) xh = -xh;
-  if (tc == 2) yh = -yh;
-  return make_float4(xh, yh, xl, yl);
+  const uint32_t tc = (uint32_t)type_class(t);
+  return make_float4(xh, yh, __uint_as_float((__float_as_uint(xl) & ~1u) | (tc & 1u)),
+                     __uint_as_float((__float_as_uint(yl) & ~1u) | (tc >> 1)));
 }
+
+// Type class carried by a float-float position (encode_ff).
+__device__ __forceinline__ uint32_t ff_class(const float4 q) {
+  return (__float_as_uint(q.z) & 1u) | ((__float_as_uint(q.w) << 1) & 2u);
+}
+
+// Packed FP32x2 arithmetic of sm_100: one instruction for the x and y lanes,
+// each lane rounded exactly as the scalar operation.
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)),
+        "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 // Cell index along one axis: v = coordinate * (n / L); NaN and negatives
 // bin to 0, v >= n to n-1 (the oracle's or_cell_bin does the same).
@@ -82,6 +102,13 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
   const float y = x - c;
   const float t = s + y;
   c = (t - s) - y;
+  s = t;
+}
+// The same for the x and y force components at once (packed FP32x2).
+__device__ __forceinline__ void kahan2(float2& s, float2& c, float2 x) {
+  const float2 y = f2sub(x, c);
+  const float2 t = f2add(s, y);
+  c = f2sub(f2sub(t, s), y);
   s = t;
 }
 
@@ -293,39 +320,33 @@ __device__ __forceinline__ DriftTail drift_tail_inputs(const Dev& D, const SysPa
 // --------------------------------------------------------- pair interaction --
 
 struct PairCtx {
-  float xih, yih, xil, yil;
-  float Lxh, Lxl, invLx, Lyh, Lyl, invLy;
+  float2 ih, il;        // slot i's float-float position (hi, lo), x and y lanes
+  float2 nLh, nLl, invL;  // -L_hi, -L_lo, 1/L_hi per axis (invL.y = 0: walled y)
   uint32_t ts;  // class whose pairs with i use the "same" parameters
   float rc2s, rc2ab, sig2s, sig2ab, e24s, e24ab, e4s, e4ab;
   float r2fs, r2fab;  // FLOOR: smallest r^2 used in the pair term (1e-5 sigma_ij^2)
   double Vcs, Vcab;
 };
 
-// Displacement i - j with the nearest image: the hi parts of two coordinates
-// in the same binade subtract exactly, the image shift s*L_hi is exact, the lo
-// parts carry the remaining bits, one rounding at the end.
+// Displacement i - j with the nearest image, x and y in the two lanes of
+// packed FP32x2 instructions: the hi parts of two coordinates in the same
+// binade subtract exactly, the image shift s*L_hi is exact, the lo parts carry
+// the remaining bits, one rounding at the end. The walled y axis of the piston
+// has invL.y = 0, which makes its shift 0.
 // MIC = false: both particles are known to sit on the same side of every
 // periodic edge (no image shift needed).
-template <bool PY, bool MIC = true>
-__device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float& dx, float& dy) {
-  float dxh = c.xih - fabsf(q.x);
-  if (!MIC) {
-    dx = dxh + (c.xil - q.z);
-    dy = (c.yih - fabsf(q.y)) + (c.yil - q.w);
-    return fmaf(dx, dx, dy * dy);
+template <bool MIC = true>
+__device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float2& d) {
+  float2 dh = f2sub(c.ih, make_float2(q.x, q.y));
+  float2 dl = f2sub(c.il, make_float2(q.z, q.w));
+  if (MIC) {
+    const float2 t = f2mul(dh, c.invL);
+    const float2 sh = make_float2(rintf(t.x), rintf(t.y));
+    dh = f2fma(sh, c.nLh, dh);
+    dl = f2fma(sh, c.nLl, dl);
   }
-  const float sx = rintf(dxh * c.invLx);
-  dxh = fmaf(-sx, c.Lxh, dxh);
-  dx = dxh + fmaf(-sx, c.Lxl, c.xil - q.z);
-  float dyh = c.yih - fabsf(q.y);
-  if (PY) {
-    const float sy = rintf(dyh * c.invLy);
-    dyh = fmaf(-sy, c.Lyh, dyh);
-    dy = dyh + fmaf(-sy, c.Lyl, c.yil - q.w);
-  } else {
-    dy = dyh + (c.yil - q.w);
-  }
-  return fmaf(dx, dx, dy * dy);
+  d = f2add(dh, dl);
+  return fmaf(d.x, d.x, d.y * d.y);
 }
 
 // The LJ pair term of li_force_kernel (src/md_cuda_common.cu:193-254) for one
@@ -333,13 +354,11 @@ __device__ __forceinline__ float pair_r2(const float4 q, const PairCtx& c, float
 // FP32 accumulation. ENERGY adds 1/2 (u_ij - V_c) in FP64 (:795-807); VIRIAL
 // adds 1/2 r.F (:676-686) as the compensated FP32 sum of tmp*r^2.
 template <bool PY, bool ENERGY, bool VIRIAL, bool MIC = true, bool FLOOR = false>
-__device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float& fxs, float& fxc,
-                                         float& fys, float& fyc, float& ws, float& wc,
-                                         double& u, double& an) {
-  float dx, dy;
-  float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
-  const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
-  const bool same = (tj == c.ts);
+__device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float2& fs, float2& fc,
+                                         float& ws, float& wc, double& u, double& an) {
+  float2 d;
+  float r2 = pair_r2<MIC>(q, c, d);
+  const bool same = (ff_class(q) == c.ts);
   const float rc2 = same ? c.rc2s : c.rc2ab;
   // 0 < r2 < rc2 for the non-negative r2 (NaN fails): bits - 1 as unsigned
   if (__float_as_uint(r2) - 1u < __float_as_uint(rc2) - 1u) {
@@ -354,8 +373,8 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
     const float sr6 = sr2 * sr2 * sr2;
     const float sr12 = sr6 * sr6;
     const float tmp = e24 * fmaf(2.0f, sr12, -sr6) * r2i;
-    kahan(fxs, fxc, tmp * dx);
-    kahan(fys, fyc, tmp * dy);
+    const float2 f = f2mul(make_float2(tmp, tmp), d);
+    kahan2(fs, fc, f);
     if (VIRIAL) kahan(ws, wc, tmp * r2);
     if (ENERGY) {
       const float e4 = same ? c.e4s : c.e4ab;
@@ -363,7 +382,7 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
       u = fma(0.5, (double)(e4 * (sr12 - sr6)) - vc, u);
       // Fx dx - Fy dy of cal_partial_U_lambda_kernel (src/md_cuda_common.cu:
       // 345-355): products of FP32 values, exact in FP64
-      an += (double)(tmp * dx) * (double)dx - (double)(tmp * dy) * (double)dy;
+      an += (double)f.x * (double)d.x - (double)f.y * (double)d.y;
     }
   }
 }
@@ -378,9 +397,9 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
 template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, bool FLOOR, typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
-                                          int li, int n, int nn, const PairCtx& c, float& fxs,
-                                          float& fxc, float& fys, float& fyc, float& ws,
-                                          float& wc, double& u, double& an) {
+                                          int li, int n, int nn, const PairCtx& c, float2& fs,
+                                          float2& fc, float& ws, float& wc, double& u,
+                                          double& an) {
   const IDX* __restrict__ p = nlist + i;
   // MIC: slot 0 of the system and a wrapped index; interior: slot i itself
   const float4* __restrict__ base = MIC ? pff + (i - li) : pff + i;
@@ -400,8 +419,7 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
     }
 #pragma unroll
     for (int q = 0; q < PF; ++q)
-      pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + j[q]), c, fxs, fxc, fys, fyc, ws, wc,
-                                               u, an);
+      pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + j[q]), c, fs, fc, ws, wc, u, an);
   }
   for (; k < nn; ++k) {
     int t = (int)__ldg(p + (int64_t)k * ntot);
@@ -410,25 +428,41 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
       t += (t < 0) ? n : 0;
       t -= (t >= n) ? n : 0;
     }
-    pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + t), c, fxs, fxc, fys, fyc, ws, wc, u, an);
+    pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + t), c, fs, fc, ws, wc, u, an);
   }
 }
 
 // Candidates j in [j0, j1) (cell stencil rows or the whole system).
 template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR>
 __device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
-                                           const PairCtx& c, float& fxs, float& fxc, float& fys,
-                                           float& fyc, float& ws, float& wc, double& u,
-                                           double& an) {
+                                           const PairCtx& c, float2& fs, float2& fc, float& ws,
+                                           float& wc, double& u, double& an) {
 #pragma unroll 4
   for (int j = j0; j < j1; ++j)
-    pair_one<PY, ENERGY, VIRIAL, true, FLOOR>(__ldg(pff + j), c, fxs, fxc, fys, fyc, ws, wc, u, an);
+    pair_one<PY, ENERGY, VIRIAL, true, FLOOR>(__ldg(pff + j), c, fs, fc, ws, wc, u, an);
 }
 
 __device__ __forceinline__ void split_box(double L, float& h, float& l, float& inv) {
   h = __double2float_rn(L);
   l = __double2float_rn(L - (double)h);
   inv = 1.0f / h;
+}
+
+// Slot i's position and the box in a pair context; PY = false leaves the y
+// image shift at 0 (walled y axis).
+template <bool PY>
+__device__ __forceinline__ void set_pair_box(PairCtx& c, const float4 qi, double Lx, double Ly) {
+  c.ih = make_float2(qi.x, qi.y);
+  c.il = make_float2(qi.z, qi.w);
+  float h, l, inv;
+  split_box(Lx, h, l, inv);
+  c.nLh.x = -h;
+  c.nLl.x = -l;
+  c.invL.x = inv;
+  split_box(Ly, h, l, inv);
+  c.nLh.y = -h;
+  c.nLl.y = -l;
+  c.invL.y = PY ? inv : 0.0f;
 }
 
 // Pair parameters of slot i's class: "same" for partners of its own class,
@@ -446,8 +480,8 @@ __device__ __forceinline__ void set_profile_class(PairCtx& c, const SysParams& P
 
 // Sum of pair forces on slot i over its 3x3 cell stencil (or every slot of the
 // system for grids narrower than 3 cells). Returns F in FP64. tci receives the
-// type class of slot i, decoded from the sign bits of its float-float
-// position (encode_ff), so the type array is not read.
+// type class of slot i, decoded from its float-float position (encode_ff), so
+// the type array is not read.
 template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR = false>
 __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
                                                int64_t i, double Lx, double Ly, double& fx,
@@ -455,13 +489,8 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
                                                int& tci) {
   PairCtx c;
   const float4 qi = __ldg(D.pff + i);
-  c.xih = fabsf(qi.x);
-  c.yih = fabsf(qi.y);
-  c.xil = qi.z;
-  c.yil = qi.w;
-  split_box(Lx, c.Lxh, c.Lxl, c.invLx);
-  split_box(Ly, c.Lyh, c.Lyl, c.invLy);
-  tci = (int)((__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u));
+  set_pair_box<PY>(c, qi, Lx, Ly);
+  tci = (int)ff_class(qi);
   c.ts = (tci == 2) ? 99u : (uint32_t)tci;
   const int sc = (tci == 2) ? 2 : tci;
   c.rc2s = P.frc2[sc];
@@ -478,7 +507,8 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
     c.r2fs = 1e-5f * P.fsig2[sc];
     c.r2fab = 1e-5f * P.fsig2[2];
   }
-  float fxs = 0.f, fxc = 0.f, fys = 0.f, fyc = 0.f, ws = 0.f, wc = 0.f;
+  float2 fs = make_float2(0.f, 0.f), fc = make_float2(0.f, 0.f);
+  float ws = 0.f, wc = 0.f;
   u = 0.0;
   an = 0.0;
   const float4* __restrict__ pff = D.pff;
@@ -488,22 +518,22 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
     const int nn = nc & (kListInterior - 1);
     if (D.nl16) {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                             fys, fyc, ws, wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+                                                  wc, u, an);
       else
-        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                            fys, fyc, ws, wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+                                                 wc, u, an);
     } else {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                             fys, fyc, ws, wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+                                                  wc, u, an);
       else
-        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fxs, fxc,
-                                            fys, fyc, ws, wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+                                                 wc, u, an);
     }
   } else if (S.allpairs) {
-    pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fxs, fxc, fys, fyc, ws,
-                                   wc, u, an);
+    pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fs, fc, ws, wc,
+                                          u, an);
   } else {
     const int ncx = S.ncx, ncy = S.ncy;
     const int cell = D.cell_of[i];
@@ -520,23 +550,23 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
       }
       const int64_t row = P.c0 + (int64_t)yy * ncx;
       if (cx > 0 && cx < ncx - 1) {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + cx - 1), __ldg(cs + row + cx + 2), c,
-                                       fxs, fxc, fys, fyc, ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + cx - 1),
+                                              __ldg(cs + row + cx + 2), c, fs, fc, ws, wc, u, an);
       } else if (cx == 0) {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fxs, fxc, fys,
-                                       fyc, ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 1), __ldg(cs + row + ncx), c,
-                                       fxs, fxc, fys, fyc, ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fs, fc,
+                                              ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 1),
+                                              __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an);
       } else {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 2), __ldg(cs + row + ncx), c,
-                                       fxs, fxc, fys, fyc, ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fxs, fxc,
-                                       fys, fyc, ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 2),
+                                              __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fs, fc,
+                                              ws, wc, u, an);
       }
     }
   }
-  fx = (double)fxs - (double)fxc;
-  fy = (double)fys - (double)fyc;
+  fx = (double)fs.x - (double)fc.x;
+  fy = (double)fs.y - (double)fc.y;
   w = 0.5 * ((double)ws - (double)wc);
 }
 
@@ -555,15 +585,14 @@ struct PairCtxD {
 template <bool PY, bool ENERGY, bool VIRIAL, bool MIC>
 __device__ __forceinline__ void pair_one_hp(const float4 q, const PairCtxD& c, double& fx,
                                             double& fy, double& w, double& u, double& an) {
-  double dx = c.xi - ((double)fabsf(q.x) + (double)q.z);
-  double dy = c.yi - ((double)fabsf(q.y) + (double)q.w);
+  double dx = c.xi - ((double)q.x + (double)q.z);
+  double dy = c.yi - ((double)q.y + (double)q.w);
   if (MIC) {
     dx = fma(-rint(dx * c.invLx), c.Lx, dx);
     if (PY) dy = fma(-rint(dy * c.invLy), c.Ly, dy);
   }
   const double r2 = fma(dx, dx, dy * dy);
-  const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
-  const bool same = (tj == c.ts);
+  const bool same = (ff_class(q) == c.ts);
   const double rc2 = same ? c.rc2s : c.rc2ab;
   if (r2 > 0.0 && r2 < rc2) {
     const double sig2 = same ? c.sig2s : c.sig2ab;
@@ -617,13 +646,13 @@ __device__ __forceinline__ void particle_force_hp(const Dev& D, const SysParams&
                                                double& u, double& an) {
   PairCtxD c;
   const float4 qi = __ldg(D.pff + i);
-  c.xi = (double)fabsf(qi.x) + (double)qi.z;
-  c.yi = (double)fabsf(qi.y) + (double)qi.w;
+  c.xi = (double)qi.x + (double)qi.z;
+  c.yi = (double)qi.y + (double)qi.w;
   c.Lx = Lx;
   c.Ly = Ly;
   c.invLx = 1.0 / Lx;
   c.invLy = 1.0 / Ly;
-  const int tci = (int)((__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u));
+  const int tci = (int)ff_class(qi);
   c.ts = (tci == 2) ? 99u : (uint32_t)tci;
   const int sc = (tci == 2) ? 2 : tci;
   const double rs = P.cutoff * P.sig[sc], rab = P.cutoff * P.sig[2];
@@ -819,7 +848,7 @@ __device__ __noinline__ ForceFinish<FM, PY> force_items_hp(Dev D, const SysParam
     if (i >= end) break;
     double fx, fy, w, u, an;
     const float4 qi = __ldg(D.pff + i);
-    const int tci = (int)((__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u));
+    const int tci = (int)ff_class(qi);
     particle_force_hp<PY, kEnergy, kVirial>(D, P, *Sp, i, Lx, Ly, fx, fy, w, u, an);
     fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
   }
@@ -1502,14 +1531,8 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
                                           int64_t k, int& nowrap) {
   PairCtx c;
   const float4 qi = D.pff[k];
-  c.xih = fabsf(qi.x);
-  c.yih = fabsf(qi.y);
-  c.xil = qi.z;
-  c.yil = qi.w;
-  split_box(S.Lx, c.Lxh, c.Lxl, c.invLx);
-  split_box(S.Ly, c.Lyh, c.Lyl, c.invLy);
-  const uint32_t tci =
-      (__float_as_uint(qi.x) >> 31) | ((__float_as_uint(qi.y) >> 30) & 2u);
+  set_pair_box<PY>(c, qi, S.Lx, S.Ly);
+  const uint32_t tci = ff_class(qi);
   const uint32_t ts = (tci == 2u) ? 99u : tci;
   const float rl2s = P.frl2[tci == 2u ? 2 : tci], rl2ab = P.frl2[2];
   const int ncx = S.ncx, ncy = S.ncy;
@@ -1550,10 +1573,9 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
       for (int j = r0[r]; j < r1[r]; ++j) {
         if (j == k) continue;
         const float4 q = D.pff[j];
-        float dx, dy;
-        const float r2 = pair_r2<PY, MIC>(q, c, dx, dy);
-        const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
-        const float rl2 = (tj == ts) ? rl2s : rl2ab;
+        float2 dd;
+        const float r2 = pair_r2<MIC>(q, c, dd);
+        const float rl2 = (ff_class(q) == ts) ? rl2s : rl2ab;
         if (r2 < rl2) {
           int d = j - (int)k;  // offset modulo n into [-n/2, n/2)
           if (d >= half) {
@@ -1665,8 +1687,6 @@ __global__ void __launch_bounds__(kThreads) k_profiles(Dev D, int s, int nb,
   const SysState& S = D.st[s];
   const double Lx = S.Lx, Ly = S.Ly;
   PairCtx c;
-  split_box(Lx, c.Lxh, c.Lxl, c.invLx);
-  split_box(Ly, c.Lyh, c.Lyl, c.invLy);
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P.n; k += stride) {
     const int64_t i = P.p0 + k;
@@ -1684,10 +1704,7 @@ __global__ void __launch_bounds__(kThreads) k_profiles(Dev D, int s, int nb,
     fix_add(ptens + nb + bk, m * v.y * v.y);
     fix_add(ptens + 2 * nb + bk, m * v.x * v.y);
     const float4 qi = D.pff[i];
-    c.xih = fabsf(qi.x);
-    c.yih = fabsf(qi.y);
-    c.xil = qi.z;
-    c.yil = qi.w;
+    set_pair_box<PY>(c, qi, Lx, Ly);
     set_profile_class(c, P, type_class(ti));
     // candidate ranges: the whole system, or the 3x3 stencil
     int r0[6], r1[6], nr = 0;
@@ -1728,10 +1745,10 @@ __global__ void __launch_bounds__(kThreads) k_profiles(Dev D, int s, int nb,
       for (int j = r0[r]; j < r1[r]; ++j) {
         if (j == i) continue;
         const float4 q = D.pff[j];
-        float dx, dy;
-        const float r2 = pair_r2<PY>(q, c, dx, dy);
-        const uint32_t tj = (__float_as_uint(q.x) >> 31) | ((__float_as_uint(q.y) >> 30) & 2u);
-        const bool same = (tj == c.ts);
+        float2 dd;
+        const float r2 = pair_r2<true>(q, c, dd);
+        const float dx = dd.x, dy = dd.y;
+        const bool same = (ff_class(q) == c.ts);
         const float rc2 = same ? c.rc2s : c.rc2ab;
         if (!(r2 > 0.0f && r2 < rc2)) continue;
         const float sig2 = same ? c.sig2s : c.sig2ab;
