@@ -31,6 +31,8 @@ constexpr int kScanBlock = 512;
 constexpr int kScanTile = kScanItems * kScanBlock;
 // ncount[] flag: the list needs neither the minimum image nor offset wrapping.
 constexpr int32_t kListInterior = 1 << 30;
+// Force phase: list rows of the next chunk prefetched into L1 per warp.
+constexpr int kListPrefetchRows = 28;
 
 // Force-phase variants.
 enum FMode : int32_t {

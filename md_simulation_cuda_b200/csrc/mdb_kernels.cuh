@@ -903,15 +903,44 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
     fin = force_items_hp<FM, PY>(D, &P, S, base, stride, end, items, Lx, Ly, h, xi2, fdt);
   } else {
     fin.init();
+    const int q_first = b - P.b0;
 #pragma unroll 1
     for (int it = 0; it < items; ++it) {
-      const int64_t i = base + (int64_t)it * stride;
-      if (skip || i >= end) break;
+      // the block's chunk of this pass (every thread of the block agrees)
+      const int q = q_first + it * P.nb;
+      const int64_t cs = P.p0 + (int64_t)q * kThreads;
+      if (skip || cs >= end) break;
+      const int64_t i = cs + threadIdx.x;
+      {
+        // L1 prefetch of the next chunk's list rows (lane r of a warp: row r
+        // of the warp's 32 slots), counts, velocities and positions, so that
+        // its dependent loads do not each wait a DRAM round trip
+        const int64_t ncs = cs + (int64_t)P.nb * kThreads;
+        const int64_t wslot = ncs + (threadIdx.x & ~31);
+        if (wslot < end) {
+          const int lane = threadIdx.x & 31;
+          if (lane < kListPrefetchRows && lane < D.max_nbr) {
+            if (D.nl16)
+              asm volatile("prefetch.global.L1 [%0];" ::"l"(D.nlist16 + (int64_t)lane * D.ntot +
+                                                             wslot));
+            else
+              asm volatile("prefetch.global.L1 [%0];" ::"l"(D.nlist + (int64_t)lane * D.ntot +
+                                                             wslot));
+          }
+          if (ncs + threadIdx.x < end) {
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(D.ncount + ncs + threadIdx.x));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(D.vel + ncs + threadIdx.x));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(D.pff + ncs + threadIdx.x));
+          }
+        }
+      }
       double fx, fy, w, u, an;
       int tci;
-      particle_force<PY, kEnergy, kVirial, kHpCapable>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an,
-                                                       tci);
-      fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
+      if (i < end) {
+        particle_force<PY, kEnergy, kVirial, kHpCapable>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an,
+                                                         tci);
+        fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
+      }
     }
   }
   if (fin.bad) atomicOr(&S->nonfinite, 1);

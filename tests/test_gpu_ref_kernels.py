@@ -88,7 +88,15 @@ def test_product_observables_vs_reference_kernels(built):
     r.close()
     sim = mdb.MDSimulation(cfg, frame=f)
     assert rel_err(sim.cal_total_U(), U_ref) < 1e-6
-    assert rel_err(sim.cal_instant_pressure(), Psum_ref / (2 * L * L)) < 1e-6
+    # the pressure is a difference of the kinetic and virial terms (about 3x
+    # cancellation); the reference's FP32 cast of the unwrapped displacement
+    # costs its periodic pairs ~1e-6 each, so both are held to the FP64 truth
+    P_ref = Psum_ref / (2 * L * L)
+    orc = po.Sim(cfg, f["pos"], f["vel"], f["type"], mode=po.OR_FP64)
+    P64 = orc.instant_pressure()
+    P = sim.cal_instant_pressure()
+    assert rel_err(P, P_ref) < 2e-5
+    assert abs(P - P64) <= abs(P_ref - P64) + 1e-7 * abs(P64)
     assert rel_err(sim.cal_partial_U_lambda(0.7), dudl_ref) < 1e-5
 
 
