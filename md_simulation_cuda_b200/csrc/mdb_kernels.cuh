@@ -323,6 +323,8 @@ struct PairCtx {
   float2 ih, il;        // slot i's float-float position (hi, lo), x and y lanes
   float2 nLh, nLl, invL;  // -L_hi, -L_lo, 1/L_hi per axis (invL.y = 0: walled y)
   uint32_t ts;  // class whose pairs with i use the "same" parameters
+  uint32_t tsz;  // pair loop: bit 0 = slot i is class 1 (B)
+  uint32_t rc2s_m1, rc2ab_m1;  // pair loop: bits of rc^2, minus 1
   float rc2s, rc2ab, sig2s, sig2ab, e24s, e24ab, e4s, e4ab;
   float r2fs, r2fab;  // FLOOR: smallest r^2 used in the pair term (1e-5 sigma_ij^2)
   double Vcs, Vcab;
@@ -358,10 +360,11 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
                                          float& ws, float& wc, double& u, double& an) {
   float2 d;
   float r2 = pair_r2<MIC>(q, c, d);
-  const bool same = (ff_class(q) == c.ts);
-  const float rc2 = same ? c.rc2s : c.rc2ab;
+  // j's class equals i's (classes 0 and 1: the lo bits of x and y are 0 / 0
+  // and 1 / 0); a class-2 slot i has its "same" parameters set to AB
+  const bool same = (((__float_as_uint(q.z) ^ c.tsz) | __float_as_uint(q.w)) & 1u) == 0u;
   // 0 < r2 < rc2 for the non-negative r2 (NaN fails): bits - 1 as unsigned
-  if (__float_as_uint(r2) - 1u < __float_as_uint(rc2) - 1u) {
+  if (__float_as_uint(r2) - 1u < (same ? c.rc2s_m1 : c.rc2ab_m1)) {
     // FLOOR (FIRE and observations): pairs closer than ~0.003 sigma (random
     // starts) take the pair term at r^2 = 1e-5 sigma^2, which keeps it finite
     // in FP32; the reference's FP32 term overflows to inf/NaN there.
@@ -492,9 +495,12 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
   set_pair_box<PY>(c, qi, Lx, Ly);
   tci = (int)ff_class(qi);
   c.ts = (tci == 2) ? 99u : (uint32_t)tci;
+  c.tsz = (tci == 1) ? 1u : 0u;
   const int sc = (tci == 2) ? 2 : tci;
   c.rc2s = P.frc2[sc];
   c.rc2ab = P.frc2[2];
+  c.rc2s_m1 = __float_as_uint(c.rc2s) - 1u;
+  c.rc2ab_m1 = __float_as_uint(c.rc2ab) - 1u;
   c.sig2s = P.fsig2[sc];
   c.sig2ab = P.fsig2[2];
   c.e24s = P.feps24[sc];
@@ -907,7 +913,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
 #pragma unroll 1
     for (int it = 0; it < items; ++it) {
       // the block's chunk of this pass (every thread of the block agrees)
-      const int q = q_first + it * P.nb;
+      // (rotated by half the blocks per pass: a block's chunks spread over
+      // the system, each pass still covering one contiguous band of chunks)
+      const int q = it * P.nb + (int)((q_first + (int64_t)it * (P.nb / 2)) % P.nb);
       const int64_t cs = P.p0 + (int64_t)q * kThreads;
       if (skip || cs >= end) break;
       const int64_t i = cs + threadIdx.x;

@@ -148,7 +148,9 @@ def test_nose_hoover_vs_reference_kernels(built):
         r.step(rk.KIND_NH, 25)
         sim.step_single_nose_hoover(nsteps=25)
         st = r.state()
-        assert abs(sim.xi - st["xi"]) < 1e-6 * (1 + abs(st["xi"]))
+        # xi integrates (2K - g T)/Q with g = 8190: 1e-7 relative differences
+        # of K (FP32 pair terms summed in different orders) add up in xi
+        assert abs(sim.xi - st["xi"]) < 1e-5 * (1 + abs(st["xi"]))
         assert rel_err(sim.cal_total_K(), r.total_K()[0]) < 1e-6
     sim.sample_collect()
     g = sim.get_host_particles()
