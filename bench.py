@@ -243,10 +243,11 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
     def steps_of(b, ids):
         return np.array([b.system_info(i)[2] for i in ids], dtype=np.int64)
 
-    b = mdb.Batch(device=dev)
+    b = mdb.Batch(device=dev, autotune=True)
     ids = [b.add_fire(cfg, f, S["force_tol"], S["max_steps"], params) for f, cfg in systems]
     t_build = time.perf_counter()
     b.run(warm_iters)
+    schedule = b.schedule()
     t_build = time.perf_counter() - t_build
     s0 = steps_of(b, ids)
     t0 = time.perf_counter()
@@ -291,6 +292,7 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
             "seconds": t_batch, "build_and_warmup_s": t_build,
             "finished_systems": done, "converged_systems": converged,
             "nonfinite_systems": int((~finite).sum()),
+            "schedule": schedule,
             "plain_path": {"value": plain, "unit": "particle-iterations/s",
                            "sample": f"{len(pick)} systems (every {max(1, len(order) // plain_sample)}"
                                      f"th by N), each alone as a batch of one, same window"},
@@ -490,7 +492,8 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     f, cfg, mode, desc = make_workload(args.workload, rank)
     N = len(f)
-    sim = mdb.MDSimulation(cfg, frame=f, device=dev)
+    sim = mdb.MDSimulation(cfg, frame=f, device=dev, autotune=True)
+    schedule = sim.schedule()
     if mode == "nh":
         step = lambda n: sim.step_single_nose_hoover(nsteps=n)  # noqa: E731
     elif mode == "nph":
@@ -641,6 +644,7 @@ def run_ours(args):
             "clocks": clk,
             "batched": batched,
             "reference_gpu": reference_gpu,
+            "schedule": schedule,
         }
         print(json.dumps(out), flush=True)
     del sim

@@ -123,12 +123,35 @@ typedef struct mdb_options {
                              FP32 pair terms throughout (stalls near 1e-6, as
                              the reference does); MDB_FIRE_FP64 uses FP64
                              pair terms from the first iteration           */
-  int32_t reserved[10];
+  int32_t autotune;       /* 1: at build, time the engine's schedule
+                             candidates on the device (list prefetch depth
+                             of the force phase, list-build grid, rebuild
+                             grid) and keep the fastest, cached per device
+                             and workload shape in the file named by
+                             MDB_SCHEDULE_CACHE (default
+                             ~/.cache/md_simulation_cuda_b200/schedule.txt).
+                             None of these changes any result bit.
+                             0 (default): the built-in schedule           */
+  int32_t reserved[9];
 } mdb_options_t;
 
 #define MDB_FIRE_AUTO 0
 #define MDB_FIRE_FP32 1
 #define MDB_FIRE_FP64 2
+
+/* The engine schedule a handle runs with (no counterpart in the reference):
+ * chosen by the autotuner (mdb_options_t.autotune) or built in. */
+typedef struct mdb_schedule {
+  int32_t list_prefetch_rows; /* force phase: next chunk's list rows per warp
+                                 prefetched into L1                         */
+  int32_t nlist_grid;         /* blocks of the list-build kernel             */
+  int32_t rebuild_grid;       /* blocks of the other rebuild kernels         */
+  int32_t items;              /* particles per thread of the largest system  */
+  int32_t tuned;              /* 1: chosen by the autotuner                  */
+  int32_t from_cache;         /* 1: read from the schedule cache file        */
+  double skin;                /* neighbour-list skin                         */
+  double tune_ms;             /* time spent timing candidates                */
+} mdb_schedule_t;
 
 /* MDConfig{} value-initialised defaults (include/md_config.hpp:14-75). */
 int mdb_config_default(mdb_config_t* out);
@@ -280,6 +303,8 @@ int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream);
  * force-phase times in milliseconds. The steps advance the simulation like
  * mdb_sim_step_*. No counterpart in the reference (which has no timers). */
 int mdb_sim_phase_times(mdb_sim_t* sim, int32_t kind, int64_t nsteps, double* ms_out);
+/* The schedule the simulation runs with (no counterpart in the reference). */
+int mdb_sim_schedule(mdb_sim_t* sim, mdb_schedule_t* out);
 /* Block until all issued work of the handle has finished. */
 int mdb_sim_synchronize(mdb_sim_t* sim);
 
@@ -448,6 +473,8 @@ int mdb_batch_partial_U_lambda_all(mdb_batch_t* b, double epsilon_lambda, double
 int mdb_batch_done_flags(mdb_batch_t* b, int32_t* done, int32_t n);
 /* Device memory the batch holds (0 before its first run). */
 int mdb_batch_device_bytes(mdb_batch_t* b, int64_t* bytes);
+/* The schedule of the batch's engine (zeros before its first run). */
+int mdb_batch_schedule(mdb_batch_t* b, mdb_schedule_t* out);
 int mdb_batch_cuda_stream(mdb_batch_t* b, void** stream);
 
 /* ---- serving: continuous batching of MD and FIRE requests ------------------
@@ -584,7 +611,11 @@ int mdb_cell_build(const double* pos, int64_t n, double Lx, double Ly, double ce
  * ordered on one stream are independent (each clears what must start at
  * zero), calls that overlap on the GPU race and give wrong results. The
  * first call on a device (with that device current) looks the array's
- * address up; make that first call before any stream capture. */
+ * address up; make that first call before any stream capture. After a
+ * cudaDeviceReset (or with another context current) the next call looks it up
+ * again. Cost: a cell holding m particles costs m^2 comparisons to order; a
+ * frame with all n particles in one cell (clustered, or non-finite positions)
+ * costs n^2 (seconds at n = 65536). */
 #define MDB_NOALLOC_MAX_PARTICLES 65536
 int mdb_compute_forces_noalloc(const mdb_config_t* cfg, const double* pos, const int32_t* type,
                                int64_t n, double Lx, double Ly, int32_t periodic_y, void* stream,

@@ -154,11 +154,12 @@ class MDSimulation:
     def __init__(self, config_manager, comm=None, filename: Optional[str] = None,
                  step: Optional[int] = None, *, frame=None, device: int = 0,
                  skin: Optional[float] = None, use_graphs: bool = True,
-                 state_file: Optional[str] = None, max_neighbors: Optional[int] = None):
+                 state_file: Optional[str] = None, max_neighbors: Optional[int] = None,
+                 autotune: bool = False):
         self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
             else MDConfigManager(_config_of(config_manager))
         self._h = C.c_void_p()
-        opt = options(device, skin, use_graphs, max_neighbors)
+        opt = options(device, skin, use_graphs, max_neighbors, autotune=autotune)
         cfg = self.cfg_manager.config
         if state_file is not None:
             # a checkpoint: frame `step` of `filename` plus the integrator state
@@ -343,6 +344,12 @@ class MDSimulation:
         check(lib().mdb_sim_cuda_stream(self._h, C.byref(p)))
         return p.value or 0
 
+    def schedule(self) -> dict:
+        """The engine schedule in use (built in, or chosen by the autotuner)."""
+        s = _lib.MDBSchedule()
+        check(lib().mdb_sim_schedule(self._h, C.byref(s)))
+        return s.as_dict()
+
 
 @dataclass
 class FireParams:
@@ -517,9 +524,10 @@ class Batch:
     (add_fire) or MD segments of one kind (add_md)."""
 
     def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True,
-                 fire_precision: Optional[int] = None):
+                 fire_precision: Optional[int] = None, autotune: bool = False):
         self._h = C.c_void_p()
-        self._opt = options(device, skin, use_graphs, fire_precision=fire_precision)
+        self._opt = options(device, skin, use_graphs, fire_precision=fire_precision,
+                            autotune=autotune)
         check(lib().mdb_batch_create(C.byref(self._opt), C.byref(self._h)))
         self._sizes = []
         self._caps = []
@@ -559,6 +567,12 @@ class Batch:
 
     def run(self, iterations: int = -1) -> None:
         check(lib().mdb_batch_run(self._h, int(iterations)))
+
+    def schedule(self) -> dict:
+        """The engine schedule of the batch (zeros before its first run)."""
+        s = _lib.MDBSchedule()
+        check(lib().mdb_batch_schedule(self._h, C.byref(s)))
+        return s.as_dict()
 
     def issue(self, iterations: int = -1) -> int:
         """Issue one chunk without waiting; returns its length."""

@@ -101,8 +101,25 @@ class MDBOptions(C.Structure):
         ("max_neighbors", C.c_int32),
         ("stream_priority", C.c_int32),
         ("fire_precision", C.c_int32),
-        ("reserved", C.c_int32 * 10),
+        ("autotune", C.c_int32),
+        ("reserved", C.c_int32 * 9),
     ]
+
+
+class MDBSchedule(C.Structure):
+    _fields_ = [
+        ("list_prefetch_rows", C.c_int32),
+        ("nlist_grid", C.c_int32),
+        ("rebuild_grid", C.c_int32),
+        ("items", C.c_int32),
+        ("tuned", C.c_int32),
+        ("from_cache", C.c_int32),
+        ("skin", C.c_double),
+        ("tune_ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class MDBObservables(C.Structure):
@@ -282,6 +299,7 @@ SIGNATURES = {
     "mdb_sim_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
     "mdb_sim_synchronize": ([_vp], C.c_int),
     "mdb_sim_phase_times": ([_vp, C.c_int32, C.c_int64, _dp], C.c_int),
+    "mdb_sim_schedule": ([_vp, C.POINTER(MDBSchedule)], C.c_int),
     "mdb_fire_params_from_config": ([_cfgp, C.POINTER(MDBFireParams)], C.c_int),
     "mdb_fire_minimize": ([_cfgp, _vp, C.c_int64, C.c_double, C.c_int32, C.POINTER(MDBFireParams),
                            _optp, _vp, C.POINTER(MDBMinimizeResult), _ip, _dp, C.c_int64], C.c_int),
@@ -303,6 +321,7 @@ SIGNATURES = {
     "mdb_batch_done_flags": ([_vp, _ip, C.c_int32], C.c_int),
     "mdb_batch_partial_U_lambda_all": ([_vp, C.c_double, _dp, C.c_int32], C.c_int),
     "mdb_batch_device_bytes": ([_vp, C.POINTER(C.c_int64)], C.c_int),
+    "mdb_batch_schedule": ([_vp, C.POINTER(MDBSchedule)], C.c_int),
     "mdb_batch_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
     "mdb_server_options_default": ([C.POINTER(MDBServerOptions)], None),
     "mdb_server_create": ([C.POINTER(MDBServerOptions), C.POINTER(_vp)], C.c_int),
@@ -365,10 +384,12 @@ FIRE_AUTO, FIRE_FP32, FIRE_FP64 = 0, 1, 2
 
 
 def options(device=0, skin=None, use_graphs=True, max_neighbors=None,
-            fire_precision=None) -> MDBOptions:
+            fire_precision=None, autotune=None) -> MDBOptions:
     o = MDBOptions()
     lib().mdb_options_default(C.byref(o))
     o.device = device
+    if autotune is not None:
+        o.autotune = 1 if autotune else 0
     if fire_precision is not None:
         o.fire_precision = int(fire_precision)
     if skin is not None:

@@ -515,6 +515,12 @@ int mdb_sim_cuda_stream(mdb_sim_t* sim, void** stream) {
   return MDB_OK;
 }
 
+int mdb_sim_schedule(mdb_sim_t* sim, mdb_schedule_t* out) {
+  if (!sim || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  *out = sim->eng->schedule();
+  return MDB_OK;
+}
+
 int mdb_sim_phase_times(mdb_sim_t* sim, int32_t kind, int64_t nsteps, double* ms_out) {
   if (!sim || !ms_out || nsteps < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
   if (kind != MDB_JOB_NVE && kind != MDB_JOB_NVT && kind != 3)
@@ -917,6 +923,13 @@ int mdb_batch_done_flags(mdb_batch_t* b, int32_t* done, int32_t n) {
   if (n != (int32_t)b->recorded_done.size())
     return mdb::set_error(MDB_ERR_CAPACITY, "n must equal the number of systems");
   for (int32_t s = 0; s < n; ++s) done[s] = b->recorded_done[s] ? 1 : 0;
+  return MDB_OK;
+}
+
+int mdb_batch_schedule(mdb_batch_t* b, mdb_schedule_t* out) {
+  if (!b || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  memset(out, 0, sizeof(*out));
+  if (b->built) *out = b->eng->schedule();
   return MDB_OK;
 }
 

@@ -3,7 +3,15 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <sys/stat.h>
+
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
 
 #include "mdb_engine.h"
 #include "mdb_kernels.cuh"
@@ -52,6 +60,7 @@ Engine::Engine(const mdb_options_t& opt) {
   max_nbr_ = opt.max_neighbors > 0 ? opt.max_neighbors : (opt.max_neighbors < 0 ? 0 : 48);
   stream_priority_ = opt.stream_priority > 0 ? opt.stream_priority : 0;
   fire_prec_ = opt.fire_precision;
+  autotune_ = opt.autotune;
   // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
   // see kernel nodes of graphs that contain conditional nodes).
   const char* eager = getenv("MDB_EAGER");
@@ -331,6 +340,7 @@ int Engine::build() {
   scan_grid_ = (int)std::min<int64_t>(ntiles, (int64_t)nsm * 4);
   scan_grid_ = std::max(scan_grid_, 1);
   D.rb_grid = rb_grid_;
+  D.pf_rows = kListPrefetchRows;
   // The list build is instruction-bound with per-slot costs that vary (list
   // lengths, minimum-image slots): one wave of resident blocks, grid-stride,
   // so that no SM is left with a partial second wave.
@@ -380,7 +390,16 @@ int Engine::build() {
       launches_ += 1;
     }
   }
-  return rebuild_now(-1);
+  rc = rebuild_now(-1);
+  if (rc) return rc;
+  int items_max = 1;
+  for (int s = 0; s < ns; ++s) items_max = std::max(items_max, (int)hsp_[s].items);
+  schedule_.list_prefetch_rows = dev_.pf_rows;
+  schedule_.nlist_grid = nlist_grid_;
+  schedule_.rebuild_grid = rb_grid_;
+  schedule_.items = items_max;
+  schedule_.skin = skin_;
+  return autotune_ ? tune() : MDB_OK;
 }
 
 int Engine::launch(void* fn, int grid, int block, const Dev& d) {
@@ -787,6 +806,187 @@ int Engine::idle(bool* out) {
     return MDB_OK;
   }
   return cuda_error(e, "cudaStreamQuery");
+}
+
+// ------------------------------------------------------------- autotuner --
+// The schedule knobs tuned here change where and when work runs, never what
+// is computed: the prefetch depth only moves list rows into L1 earlier, and
+// the rebuild kernels are grid-stride loops over independent slots and cells
+// whose order is fixed by the stable sort. Candidates are timed on state-
+// neutral work: FM_INIT launches recompute the accelerations the state
+// already holds, and a rebuild at unchanged positions keeps every slot where
+// it is (the sort is stable and the cells are unchanged).
+namespace {
+
+std::mutex g_cache_mu;
+
+std::string cache_path() {
+  const char* p = getenv("MDB_SCHEDULE_CACHE");
+  if (p && p[0]) return p;
+  const char* home = getenv("HOME");
+  const std::string dir = std::string(home && home[0] ? home : "/tmp") + "/.cache";
+  mkdir(dir.c_str(), 0755);
+  const std::string d2 = dir + "/md_simulation_cuda_b200";
+  mkdir(d2.c_str(), 0755);
+  return d2 + "/schedule.txt";
+}
+
+bool cache_lookup(const std::string& key, int* pf, int* nlg, int* rbg) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  std::ifstream in(cache_path());
+  if (!in) return false;
+  std::string line;
+  bool found = false;
+  while (std::getline(in, line)) {
+    const size_t tab = line.find('\t');
+    if (tab == std::string::npos || line.compare(0, tab, key) != 0 || tab != key.size()) continue;
+    std::istringstream vs(line.substr(tab + 1));
+    int a, b, c;
+    if (vs >> a >> b >> c) {
+      *pf = a;
+      *nlg = b;
+      *rbg = c;
+      found = true;  // the last entry for the key wins
+    }
+  }
+  return found;
+}
+
+void cache_store(const std::string& key, int pf, int nlg, int rbg) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  std::ofstream out(cache_path(), std::ios::app);
+  if (out) out << key << '\t' << pf << ' ' << nlg << ' ' << rbg << '\n';
+}
+
+int bucket(int64_t x) {  // log2 bucket of a size
+  int b = 0;
+  while (x > 1) {
+    x >>= 1;
+    ++b;
+  }
+  return b;
+}
+
+}  // namespace
+
+int Engine::time_force_init(int reps, double* ms) {
+  cudaEvent_t a, b;
+  MDB_CUDA(cudaEventCreate(&a));
+  MDB_CUDA(cudaEventCreate(&b));
+  int rc = launch(force_fn(FM_INIT, true), nblocks_, kThreads, dev_);  // warm
+  double best = 1e30;
+  for (int r = 0; !rc && r < reps; ++r) {
+    cudaEventRecord(a, stream_);
+    rc = launch(force_fn(FM_INIT, true), nblocks_, kThreads, dev_);
+    cudaEventRecord(b, stream_);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    best = std::min(best, (double)t);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return rc;
+}
+
+int Engine::time_rebuild(int reps, double* ms) {
+  cudaEvent_t a, b;
+  MDB_CUDA(cudaEventCreate(&a));
+  MDB_CUDA(cudaEventCreate(&b));
+  int rc = rebuild_now(-1);  // warm
+  double best = 1e30;
+  for (int r = 0; !rc && r < reps; ++r) {
+    cudaEventRecord(a, stream_);
+    rc = rebuild_now(-1);
+    cudaEventRecord(b, stream_);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    best = std::min(best, (double)t);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return rc;
+}
+
+int Engine::tune() {
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaDeviceProp prop;
+  MDB_CUDA(cudaGetDeviceProperties(&prop, device_));
+  const int nsm = prop.multiProcessorCount;
+  int kinds = 0;
+  for (const SystemSpec& sp : specs_) kinds |= 1 << sp.kind;
+  char keyb[512];
+  snprintf(keyb, sizeof(keyb), "%s|sm%d|sys%d|n%d|cells%d|nbr%d|nl16_%d|skin%.3f|kinds%d",
+           prop.name, nsm, bucket((int64_t)specs_.size()), bucket(ntot_), bucket(ncells_),
+           max_nbr_, dev_.nl16, skin_, kinds);
+  const std::string key(keyb);
+  int pf = dev_.pf_rows, nlg = nlist_grid_, rbg = rb_grid_;
+  if (cache_lookup(key, &pf, &nlg, &rbg)) {
+    dev_.pf_rows = pf;
+    nlist_grid_ = std::max(1, nlg);
+    rb_grid_ = std::max(1, rbg);
+    dev_.rb_grid = rb_grid_;
+    schedule_.from_cache = 1;
+  } else {
+    // force phase: list prefetch depth
+    double best = 1e30;
+    int best_pf = dev_.pf_rows;
+    for (int cand : {0, 8, 16, 28}) {
+      dev_.pf_rows = cand;
+      double ms = 0.0;
+      const int rc = time_force_init(3, &ms);
+      if (rc) return rc;
+      if (ms < best * 0.98) {  // prefer the earlier (smaller) choice within 2%
+        best = ms;
+        best_pf = cand;
+      }
+    }
+    dev_.pf_rows = best_pf;
+    // rebuild: list-build grid, then the grid of the other rebuild kernels
+    const int one_wave = nlist_grid_;
+    const int64_t work = std::max(ntot_, ncells_);
+    const int cap = (int)std::max<int64_t>(1, (work + kThreads - 1) / kThreads);
+    best = 1e30;
+    int best_nlg = one_wave;
+    for (int cand : {one_wave, std::min(cap, 2 * one_wave), std::max(1, one_wave / 2)}) {
+      nlist_grid_ = cand;
+      double ms = 0.0;
+      const int rc = time_rebuild(2, &ms);
+      if (rc) return rc;
+      if (ms < best * 0.98) {
+        best = ms;
+        best_nlg = cand;
+      }
+    }
+    nlist_grid_ = best_nlg;
+    best = 1e30;
+    int best_rbg = rb_grid_;
+    for (int cand : {rb_grid_, std::min(cap, nsm * 16), std::min(cap, nsm * 4)}) {
+      rb_grid_ = std::max(1, cand);
+      dev_.rb_grid = rb_grid_;
+      double ms = 0.0;
+      const int rc = time_rebuild(2, &ms);
+      if (rc) return rc;
+      if (ms < best * 0.98) {
+        best = ms;
+        best_rbg = rb_grid_;
+      }
+    }
+    rb_grid_ = best_rbg;
+    dev_.rb_grid = rb_grid_;
+    cache_store(key, dev_.pf_rows, nlist_grid_, rb_grid_);
+  }
+  MDB_CUDA(cudaStreamSynchronize(stream_));
+  schedule_.list_prefetch_rows = dev_.pf_rows;
+  schedule_.nlist_grid = nlist_grid_;
+  schedule_.rebuild_grid = rb_grid_;
+  schedule_.tuned = 1;
+  schedule_.tune_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return MDB_OK;
 }
 
 }  // namespace mdb

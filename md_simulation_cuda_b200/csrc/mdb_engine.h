@@ -82,6 +82,8 @@ class Engine {
   int idle(bool* out);
   // Device memory the engine holds, in bytes.
   int64_t device_bytes() const { return bytes_; }
+  // The schedule in use (built in, or chosen by the autotuner at build).
+  const mdb_schedule_t& schedule() const { return schedule_; }
 
   // Kernel launches issued (eager launches + kernel nodes of launched graphs,
   // counting the rebuild body once per rebuild actually run).
@@ -97,6 +99,12 @@ class Engine {
   int add_cond_rebuild(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
                        cudaGraphNode_t* out);
   int get_graph(int kind, int dm, int fm, bool py, int chunk, cudaGraphExec_t* exec);
+  // Times the schedule candidates on the built state (every candidate leaves
+  // the state bit for bit as it was) and keeps the fastest; cached per device
+  // and workload shape.
+  int tune();
+  int time_force_init(int reps, double* ms);
+  int time_rebuild(int reps, double* ms);
   void drop_graphs();
 
   int device_ = 0;
@@ -114,6 +122,8 @@ class Engine {
   int scan_grid_ = 0;
   int nlist_grid_ = 0;
   int fire_prec_ = MDB_FIRE_AUTO;
+  int autotune_ = 0;
+  mdb_schedule_t schedule_{};
   int stream_priority_ = 0;  // levels above normal for stream_  // k_rb_nlist: one wave of resident blocks
   int64_t aos_cap_ = 0;
   void* d_aos_ = nullptr;

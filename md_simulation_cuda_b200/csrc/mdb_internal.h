@@ -31,7 +31,8 @@ constexpr int kScanBlock = 512;
 constexpr int kScanTile = kScanItems * kScanBlock;
 // ncount[] flag: the list needs neither the minimum image nor offset wrapping.
 constexpr int32_t kListInterior = 1 << 30;
-// Force phase: list rows of the next chunk prefetched into L1 per warp.
+// Force phase: list rows of the next chunk prefetched into L1 per warp
+// (built-in schedule; Dev::pf_rows holds the one in use).
 constexpr int kListPrefetchRows = 28;
 
 // Force-phase variants.
@@ -147,6 +148,7 @@ struct Dev {
   cudaGraphConditionalHandle cond;
   int32_t use_cond;
   int32_t rb_grid;    // grid of the grid-stride rebuild kernels
+  int32_t pf_rows;    // force phase: list rows of the next chunk prefetched per warp
 };
 
 }  // namespace mdb

@@ -927,7 +927,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
         const int64_t wslot = ncs + (threadIdx.x & ~31);
         if (wslot < end) {
           const int lane = threadIdx.x & 31;
-          if (lane < kListPrefetchRows && lane < D.max_nbr) {
+          if (lane < D.pf_rows && lane < D.max_nbr) {
             if (D.nl16)
               asm volatile("prefetch.global.L1 [%0];" ::"l"(D.nlist16 + (int64_t)lane * D.ntot +
                                                              wslot));

@@ -16,7 +16,17 @@
 // MDB_NOALLOC_MAX_PARTICLES particles, and at most 128 x 128 cells (larger
 // boxes use wider cells, which stays exact). The first call on each device
 // looks the array's address up with cudaGetSymbolAddress while that device
-// is current; make that first call before any stream capture.
+// is current; make that first call before any stream capture. The address is
+// remembered together with the CUDA context it belongs to: after a
+// cudaDeviceReset, or with another context current on the device, the next
+// call looks it up again instead of using a stale address.
+//
+// Cost: the order inside a cell is each particle's rank among the cell's
+// indices, found by a scan of the cell, so a cell holding m particles costs
+// m^2 comparisons. Ordinary frames hold a few particles per cell; a frame
+// with all particles in a few cells (clustered input, or non-finite positions,
+// which all bin to cell 0) costs up to n^2, about 4e9 comparisons (seconds)
+// at n = 65536.
 //
 // Every call on a device shares the one array: each call first clears the
 // parts that must start at zero (the per-cell counts and the arrival counter)
@@ -29,10 +39,10 @@
 // truncated force and the shifted energy of the other force paths, FP64
 // accumulation in a fixed order (cells in stencil order, particles in index
 // order inside a cell), so a call is deterministic.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 
-#include <atomic>
 #include <mutex>
 
 #include "mdb200.h"
@@ -272,26 +282,55 @@ __global__ void __launch_bounds__(kNaThreads) k_na_force(const double* __restric
 
 std::mutex g_setup_mu;
 constexpr int kMaxDevices = 64;
-std::atomic<unsigned char*> g_scratch_ptr[kMaxDevices];
+struct ScratchAddr {
+  CUcontext ctx = nullptr;
+  unsigned char* ptr = nullptr;
+};
+ScratchAddr g_scratch[kMaxDevices];  // guarded by g_setup_mu
 
-// Once per device, with that device current: the device address of the
-// scratch array.
+// cuCtxGetCurrent through the runtime's driver entry point (no link against
+// the driver library).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  return fn;
+}
+
+// Once per device and context, with that device current: the device address
+// of the scratch array.
 int scratch_for_device(int dev, unsigned char** out) {
   if (dev < 0 || dev >= kMaxDevices)
     return set_error(MDB_ERR_ARG, "mdb_compute_forces_noalloc: device ordinal out of range");
-  unsigned char* p = g_scratch_ptr[dev].load(std::memory_order_acquire);
-  if (!p) {
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    p = g_scratch_ptr[dev].load(std::memory_order_relaxed);
-    if (!p) {
-      void* addr = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-      if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-      p = static_cast<unsigned char*>(addr);
-      g_scratch_ptr[dev].store(p, std::memory_order_release);
-    }
+  CtxGetCurrentFn get = ctx_get_current();
+  CUcontext ctx = nullptr;
+  if (!get || get(&ctx) != CUDA_SUCCESS)
+    return set_error(MDB_ERR_CUDA, "mdb_compute_forces_noalloc: cuCtxGetCurrent failed");
+  std::lock_guard<std::mutex> lk(g_setup_mu);
+  if (!ctx) {
+    // no context yet on this thread: the runtime's first call makes the
+    // device's primary context current
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    if (get(&ctx) != CUDA_SUCCESS || !ctx)
+      return set_error(MDB_ERR_CUDA, "mdb_compute_forces_noalloc: no current CUDA context");
   }
-  *out = p;
+  ScratchAddr& a = g_scratch[dev];
+  if (a.ptr == nullptr || a.ctx != ctx) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    a.ptr = static_cast<unsigned char*>(addr);
+    a.ctx = ctx;
+  }
+  *out = a.ptr;
   return MDB_OK;
 }
 

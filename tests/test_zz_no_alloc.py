@@ -88,3 +88,76 @@ def test_noalloc_rejects_sizes_beyond_the_maximum(built):
                                                p)
     assert rc == _lib.MDB_ERR_CAPACITY
     assert "MDB_NOALLOC_MAX_PARTICLES" in _lib.last_error()
+
+
+def test_noalloc_empty_frame_writes_zero_energies(built):
+    """n = 0: nothing to evaluate, U and W are written as 0."""
+    import torch
+
+    uw = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    cfg = mdb._config_of(wl.config_dict(1, 10.0, 10.0, dt=0.001))
+    rc = _lib.lib().mdb_compute_forces_noalloc(C.byref(cfg), None, None, 0, 10.0, 10.0, 1, None,
+                                               None, C.c_void_p(uw.data_ptr()))
+    assert rc == _lib.MDB_OK, _lib.last_error()
+    torch.cuda.synchronize()
+    assert uw.cpu().numpy().tolist() == [0.0, 0.0]
+
+
+def test_noalloc_streams_ordered_by_an_event(built):
+    """Two calls on two streams, the second waiting on an event recorded after
+    the first: the same results as two calls on one stream."""
+    import torch
+
+    f1, cfg1 = wl.nve_4096(seed=4)
+    f2, cfg2 = wl.nve_4096(seed=6)
+    ref1 = _noalloc(cfg1, f1, cfg1["box_w_global"], cfg1["box_h_global"])
+    ref2 = _noalloc(cfg2, f2, cfg2["box_w_global"], cfg2["box_h_global"])
+    dev = torch.device("cuda", 0)
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    outs = []
+    ev = torch.cuda.Event()
+    for k, (f, cfg, st) in enumerate(((f1, cfg1, s1), (f2, cfg2, s2))):
+        pos = torch.from_numpy(np.ascontiguousarray(f["pos"])).to(dev)
+        typ = torch.from_numpy(np.ascontiguousarray(f["type"], dtype=np.int32)).to(dev)
+        acc = torch.full((len(f), 2), float("nan"), dtype=torch.float64, device=dev)
+        uw = torch.full((2,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        if k == 1:
+            st.wait_event(ev)
+        rc = _lib.lib().mdb_compute_forces_noalloc(
+            C.byref(mdb._config_of(cfg)), C.c_void_p(pos.data_ptr()),
+            C.c_void_p(typ.data_ptr()), len(f), cfg["box_w_global"], cfg["box_h_global"], 1,
+            C.c_void_p(st.cuda_stream), C.c_void_p(acc.data_ptr()), C.c_void_p(uw.data_ptr()))
+        assert rc == _lib.MDB_OK, _lib.last_error()
+        if k == 0:
+            ev.record(st)
+        outs.append((acc, uw, pos, typ))
+    torch.cuda.synchronize(dev)
+    for (acc, uw, _, _), ref in zip(outs, (ref1, ref2)):
+        assert np.array_equal(acc.cpu().numpy(), ref[0])
+        assert uw.cpu().numpy().tolist() == [ref[1], ref[2]]
+
+
+def test_noalloc_allocates_nothing(built):
+    """Warm calls leave the device's free memory unchanged."""
+    import torch
+
+    f, cfg = wl.nve_4096(seed=2)
+    L = cfg["box_w_global"]
+    _noalloc(cfg, f, L, L)  # warm: device set-up, torch's own buffers
+    dev = torch.device("cuda", 0)
+    pos = torch.from_numpy(np.ascontiguousarray(f["pos"])).to(dev)
+    typ = torch.from_numpy(np.ascontiguousarray(f["type"], dtype=np.int32)).to(dev)
+    acc = torch.empty((len(f), 2), dtype=torch.float64, device=dev)
+    uw = torch.empty((2,), dtype=torch.float64, device=dev)
+    c = mdb._config_of(cfg)
+    torch.cuda.synchronize(dev)
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(5):
+        rc = _lib.lib().mdb_compute_forces_noalloc(
+            C.byref(c), C.c_void_p(pos.data_ptr()), C.c_void_p(typ.data_ptr()), len(f), L, L, 1,
+            None, C.c_void_p(acc.data_ptr()), C.c_void_p(uw.data_ptr()))
+        assert rc == _lib.MDB_OK, _lib.last_error()
+    torch.cuda.synchronize(dev)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
