@@ -812,10 +812,12 @@ int Engine::idle(bool* out) {
 // The schedule knobs tuned here change where and when work runs, never what
 // is computed: the prefetch depth only moves list rows into L1 earlier, and
 // the rebuild kernels are grid-stride loops over independent slots and cells
-// whose order is fixed by the stable sort. Candidates are timed on state-
-// neutral work: FM_INIT launches recompute the accelerations the state
-// already holds, and a rebuild at unchanged positions keeps every slot where
-// it is (the sort is stable and the cells are unchanged).
+// whose order is fixed by the stable sort. Candidates are timed on the
+// workload's own force phase (Nose-Hoover for MD handles, FIRE for FIRE
+// batches), after which the velocities, accelerations and every system's
+// scalar state are put back (positions do not move), and on rebuilds at
+// unchanged positions, which keep every slot where it is (the sort is stable
+// and the cells are unchanged).
 namespace {
 
 std::mutex g_cache_mu;
@@ -869,15 +871,15 @@ int bucket(int64_t x) {  // log2 bucket of a size
 
 }  // namespace
 
-int Engine::time_force_init(int reps, double* ms) {
+int Engine::time_force(int fm, int reps, double* ms) {
   cudaEvent_t a, b;
   MDB_CUDA(cudaEventCreate(&a));
   MDB_CUDA(cudaEventCreate(&b));
-  int rc = launch(force_fn(FM_INIT, true), nblocks_, kThreads, dev_);  // warm
+  int rc = launch(force_fn(fm, true), nblocks_, kThreads, dev_);  // warm
   double best = 1e30;
   for (int r = 0; !rc && r < reps; ++r) {
     cudaEventRecord(a, stream_);
-    rc = launch(force_fn(FM_INIT, true), nblocks_, kThreads, dev_);
+    rc = launch(force_fn(fm, true), nblocks_, kThreads, dev_);
     cudaEventRecord(b, stream_);
     cudaEventSynchronize(b);
     float t = 0.f;
@@ -931,20 +933,36 @@ int Engine::tune() {
     dev_.rb_grid = rb_grid_;
     schedule_.from_cache = 1;
   } else {
-    // force phase: list prefetch depth
+    // force phase: list prefetch depth, timed on the workload's force kernel
+    // with the velocities (kicked by it) and the scalar state put back after
+    const bool all_fire = (kinds == (1 << K_FIRE));
+    const int fm = all_fire ? FM_FIRE : FM_NH;
+    std::vector<SysState> snap;
+    if (int rc = get_states(snap)) return rc;
+    MDB_CUDA(cudaMemcpyAsync(dev_.vel2, dev_.vel, sizeof(double2) * (size_t)ntot_,
+                             cudaMemcpyDeviceToDevice, stream_));
+    MDB_CUDA(cudaMemcpyAsync(dev_.acc2, dev_.acc, sizeof(double2) * (size_t)ntot_,
+                             cudaMemcpyDeviceToDevice, stream_));
     double best = 1e30;
     int best_pf = dev_.pf_rows;
-    for (int cand : {0, 8, 16, 28}) {
+    for (int cand : {28, 16, 8, 0}) {
       dev_.pf_rows = cand;
       double ms = 0.0;
-      const int rc = time_force_init(3, &ms);
+      const int rc = time_force(fm, 3, &ms);
       if (rc) return rc;
-      if (ms < best * 0.98) {  // prefer the earlier (smaller) choice within 2%
+      if (ms < best * 0.98) {  // keep the earlier (deeper) choice within 2%
         best = ms;
         best_pf = cand;
       }
     }
     dev_.pf_rows = best_pf;
+    MDB_CUDA(cudaMemcpyAsync(dev_.vel, dev_.vel2, sizeof(double2) * (size_t)ntot_,
+                             cudaMemcpyDeviceToDevice, stream_));
+    MDB_CUDA(cudaMemcpyAsync(dev_.acc, dev_.acc2, sizeof(double2) * (size_t)ntot_,
+                             cudaMemcpyDeviceToDevice, stream_));
+    MDB_CUDA(cudaMemcpyAsync(dev_.st, snap.data(), sizeof(SysState) * snap.size(),
+                             cudaMemcpyHostToDevice, stream_));
+    MDB_CUDA(cudaStreamSynchronize(stream_));
     // rebuild: list-build grid, then the grid of the other rebuild kernels
     const int one_wave = nlist_grid_;
     const int64_t work = std::max(ntot_, ncells_);

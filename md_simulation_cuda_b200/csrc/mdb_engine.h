@@ -103,7 +103,7 @@ class Engine {
   // the state bit for bit as it was) and keeps the fastest; cached per device
   // and workload shape.
   int tune();
-  int time_force_init(int reps, double* ms);
+  int time_force(int fm, int reps, double* ms);
   int time_rebuild(int reps, double* ms);
   void drop_graphs();
 
