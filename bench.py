@@ -66,20 +66,6 @@ def max_over_ranks(x: float, dist, device) -> float:
     return float(t.item())
 
 
-def lpt_assign(costs, nbins):
-    """Greedy longest-processing-time assignment of independent systems to
-    ranks: largest cost first, each to the least-loaded rank (ties to the
-    lower rank). Returns the rank of every system."""
-    order = sorted(range(len(costs)), key=lambda k: (-costs[k], k))
-    load = [0.0] * nbins
-    out = [0] * len(costs)
-    for k in order:
-        r = min(range(nbins), key=lambda b: (load[b], b))
-        out[k] = r
-        load[r] += costs[k]
-    return out
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -234,9 +220,11 @@ def measure_fire_mix(dev, warm_iters, iters, plain_sample=32, to_completion=Fals
     S = wl.FIRE_SETTINGS
     params = wl.fire_params()
     systems = wl.fire_mix(512)
-    if shard is not None:  # this rank's systems (LPT by N, no collective on the data path)
+    if shard is not None:
+        # this rank's systems: the library's LPT placement on particles x
+        # iteration cap (the same on every rank; no collective on the data path)
         rank, ws = shard
-        owner = lpt_assign([len(f) for f, _ in systems], ws)
+        owner, _ = mdb.place_lpt([len(f) * S["max_steps"] for f, _ in systems], ws)
         systems = [x for x, r in zip(systems, owner) if r == rank]
     sizes = np.array([len(f) for f, _ in systems])
 

@@ -475,6 +475,43 @@ int mdb_batch_done_flags(mdb_batch_t* b, int32_t* done, int32_t n);
 int mdb_batch_device_bytes(mdb_batch_t* b, int64_t* bytes);
 /* The schedule of the batch's engine (zeros before its first run). */
 int mdb_batch_schedule(mdb_batch_t* b, mdb_schedule_t* out);
+
+/* ---- independent systems over several GPUs (no counterpart in the reference,
+ * which runs one system per job: scripts/submit_batches_*.sh) --------------
+ * mdb_place_lpt: the greedy longest-processing-time placement of n items of
+ * the given costs on nbins bins (largest cost first, each to the least-loaded
+ * bin, ties to the lower bin); bin_out[n], load_out[nbins] (optional).
+ * A multi-device batch takes systems like mdb_batch_* (one kind per batch),
+ * places them at its first run by that rule on particles x steps (FIRE: the
+ * iteration cap) over `devices` (a device may be listed more than once), and
+ * runs one batch per device concurrently from the calling thread. No data
+ * crosses devices; each system's results equal its results alone. */
+int mdb_place_lpt(const double* costs, int32_t n, int32_t nbins, int32_t* bin_out,
+                  double* load_out);
+typedef struct mdb_multibatch mdb_multibatch_t;
+int mdb_multibatch_create(const mdb_options_t* opt, const int32_t* devices, int32_t ndev,
+                          mdb_multibatch_t** out);
+int mdb_multibatch_destroy(mdb_multibatch_t* m);
+int mdb_multibatch_add_fire(mdb_multibatch_t* m, const mdb_config_t* cfg,
+                            const mdb_particle_t* frame, int64_t n, double force_tol,
+                            int32_t max_steps, const mdb_fire_params_t* params, int32_t* sys_id);
+int mdb_multibatch_add_md(mdb_multibatch_t* m, const mdb_config_t* cfg,
+                          const mdb_particle_t* frame, int64_t n, int32_t kind, int64_t nsteps,
+                          int32_t* sys_id);
+/* Advance every system by up to `iterations` (< 0: until all are finished). */
+int mdb_multibatch_run(mdb_multibatch_t* m, int64_t iterations);
+/* The device each system was placed on (n = number of systems). */
+int mdb_multibatch_placement(mdb_multibatch_t* m, int32_t* device_of, int32_t n);
+int mdb_multibatch_progress(mdb_multibatch_t* m, int32_t* n_systems, int32_t* n_done);
+int mdb_multibatch_system_info(mdb_multibatch_t* m, int32_t sys_id, int64_t* n, int32_t* done,
+                               int64_t* steps);
+int mdb_multibatch_get_frame(mdb_multibatch_t* m, int32_t sys_id, mdb_particle_t* out,
+                             int64_t n);
+int mdb_multibatch_get_fire_result(mdb_multibatch_t* m, int32_t sys_id,
+                                   mdb_minimize_result_t* result, int32_t* energy_steps,
+                                   double* energy_trace, int64_t trace_cap);
+int mdb_multibatch_energies(mdb_multibatch_t* m, int32_t sys_id, double* K, double* U,
+                            double* xi);
 int mdb_batch_cuda_stream(mdb_batch_t* b, void** stream);
 
 /* ---- serving: continuous batching of MD and FIRE requests ------------------

@@ -650,6 +650,113 @@ class Batch:
         return p.value or 0
 
 
+def place_lpt(costs, nbins: int):
+    """Greedy longest-processing-time placement (mdb_place_lpt): the bin of
+    every item and the load of every bin."""
+    c = np.ascontiguousarray(costs, dtype=np.float64)
+    out = np.zeros(len(c), dtype=np.int32)
+    load = np.zeros(nbins, dtype=np.float64)
+    check(lib().mdb_place_lpt(c.ctypes.data_as(C.POINTER(C.c_double)), len(c), int(nbins),
+                              out.ctypes.data_as(C.POINTER(C.c_int32)),
+                              load.ctypes.data_as(C.POINTER(C.c_double))))
+    return out, load
+
+
+class MultiBatch:
+    """Independent systems over several GPUs (mdb_multibatch_*): placed at the
+    first run by longest-processing-time on particles x steps, one batch per
+    device, run concurrently; a device may be listed more than once."""
+
+    def __init__(self, devices=(0,), skin: Optional[float] = None, use_graphs: bool = True,
+                 fire_precision: Optional[int] = None, autotune: bool = False):
+        self._h = C.c_void_p()
+        self._opt = options(0, skin, use_graphs, fire_precision=fire_precision,
+                            autotune=autotune)
+        dv = np.ascontiguousarray(list(devices), dtype=np.int32)
+        check(lib().mdb_multibatch_create(C.byref(self._opt),
+                                          dv.ctypes.data_as(C.POINTER(C.c_int32)), len(dv),
+                                          C.byref(self._h)))
+        self._sizes = []
+        self._caps = []
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._h = None
+            try:
+                lib().mdb_multibatch_destroy(h)
+            except Exception:
+                pass
+
+    def add_fire(self, config, frame, force_tol: float, max_steps: int,
+                 params: FireParams) -> int:
+        f = _as_frame(frame)
+        sid = C.c_int32()
+        p = params._c()
+        check(lib().mdb_multibatch_add_fire(self._h, C.byref(_config_of(config)), frame_ptr(f),
+                                            len(f), float(force_tol), int(max_steps),
+                                            C.byref(p), C.byref(sid)))
+        self._sizes.append(len(f))
+        self._caps.append(max_steps // 1000 + 4)
+        return sid.value
+
+    def add_md(self, config, frame, kind: int, nsteps: int) -> int:
+        f = _as_frame(frame)
+        sid = C.c_int32()
+        check(lib().mdb_multibatch_add_md(self._h, C.byref(_config_of(config)), frame_ptr(f),
+                                          len(f), int(kind), int(nsteps), C.byref(sid)))
+        self._sizes.append(len(f))
+        self._caps.append(4)
+        return sid.value
+
+    def run(self, iterations: int = -1) -> None:
+        check(lib().mdb_multibatch_run(self._h, int(iterations)))
+
+    def placement(self) -> np.ndarray:
+        out = np.zeros(len(self._sizes), dtype=np.int32)
+        check(lib().mdb_multibatch_placement(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)),
+                                             len(out)))
+        return out
+
+    def progress(self):
+        a, b = C.c_int32(), C.c_int32()
+        check(lib().mdb_multibatch_progress(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def system_info(self, sys_id: int):
+        n, d, st = C.c_int64(), C.c_int32(), C.c_int64()
+        check(lib().mdb_multibatch_system_info(self._h, sys_id, C.byref(n), C.byref(d),
+                                               C.byref(st)))
+        return n.value, bool(d.value), st.value
+
+    def energies(self, sys_id: int):
+        K, U, xi = C.c_double(), C.c_double(), C.c_double()
+        check(lib().mdb_multibatch_energies(self._h, sys_id, C.byref(K), C.byref(U),
+                                            C.byref(xi)))
+        return K.value, U.value, xi.value
+
+    def frame(self, sys_id: int) -> np.ndarray:
+        f = make_frame(self._sizes[sys_id])
+        check(lib().mdb_multibatch_get_frame(self._h, sys_id, frame_ptr(f), len(f)))
+        return f
+
+    def fire_result(self, sys_id: int, with_frame: bool = True) -> MinimizeResult:
+        res = MDBMinimizeResult()
+        cap = self._caps[sys_id]
+        es = np.zeros(cap, dtype=np.int32)
+        et = np.zeros(cap, dtype=np.float64)
+        check(lib().mdb_multibatch_get_fire_result(self._h, sys_id, C.byref(res),
+                                                   es.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                   et.ctypes.data_as(C.POINTER(C.c_double)),
+                                                   cap))
+        k = min(res.n_energy_samples, cap)
+        return MinimizeResult(frame=self.frame(sys_id) if with_frame else make_frame(0),
+                              energy_steps=es[:k].tolist(), energy_trace=et[:k].tolist(),
+                              steps=res.steps, converged=bool(res.converged),
+                              max_force=res.max_force, potential_energy=res.potential_energy,
+                              nonfinite=bool(res.nonfinite))
+
+
 @dataclass
 class RequestResult:
     """A finished request of a Server."""

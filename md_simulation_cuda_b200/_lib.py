@@ -322,6 +322,21 @@ SIGNATURES = {
     "mdb_batch_partial_U_lambda_all": ([_vp, C.c_double, _dp, C.c_int32], C.c_int),
     "mdb_batch_device_bytes": ([_vp, C.POINTER(C.c_int64)], C.c_int),
     "mdb_batch_schedule": ([_vp, C.POINTER(MDBSchedule)], C.c_int),
+    "mdb_place_lpt": ([_dp, C.c_int32, C.c_int32, _ip, _dp], C.c_int),
+    "mdb_multibatch_create": ([_optp, _ip, C.c_int32, C.POINTER(_vp)], C.c_int),
+    "mdb_multibatch_destroy": ([_vp], C.c_int),
+    "mdb_multibatch_add_fire": ([_vp, _cfgp, _vp, C.c_int64, C.c_double, C.c_int32,
+                                 C.POINTER(MDBFireParams), _ip], C.c_int),
+    "mdb_multibatch_add_md": ([_vp, _cfgp, _vp, C.c_int64, C.c_int32, C.c_int64, _ip], C.c_int),
+    "mdb_multibatch_run": ([_vp, C.c_int64], C.c_int),
+    "mdb_multibatch_placement": ([_vp, _ip, C.c_int32], C.c_int),
+    "mdb_multibatch_progress": ([_vp, _ip, _ip], C.c_int),
+    "mdb_multibatch_system_info": ([_vp, C.c_int32, C.POINTER(C.c_int64), _ip,
+                                    C.POINTER(C.c_int64)], C.c_int),
+    "mdb_multibatch_get_frame": ([_vp, C.c_int32, _vp, C.c_int64], C.c_int),
+    "mdb_multibatch_get_fire_result": ([_vp, C.c_int32, C.POINTER(MDBMinimizeResult), _ip, _dp,
+                                        C.c_int64], C.c_int),
+    "mdb_multibatch_energies": ([_vp, C.c_int32, _dp, _dp, _dp], C.c_int),
     "mdb_batch_cuda_stream": ([_vp, C.POINTER(_vp)], C.c_int),
     "mdb_server_options_default": ([C.POINTER(MDBServerOptions)], None),
     "mdb_server_create": ([C.POINTER(MDBServerOptions), C.POINTER(_vp)], C.c_int),

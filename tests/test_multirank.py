@@ -1,6 +1,7 @@
-"""The multi-rank host logic of bench.py on CPU ranks (gloo, world size 2):
-the max-over-ranks timing, the LPT sharding of independent systems (each
-system on exactly one rank, loads balanced), and per-rank replica seeds."""
+"""The multi-rank host logic on CPU ranks (gloo, world size 2): bench.py's
+max-over-ranks timing, the library's LPT placement of independent systems
+(mdb_place_lpt: each system on exactly one rank, loads balanced, the same on
+every rank), and per-rank replica seeds."""
 import os
 import socket
 
@@ -10,6 +11,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 import bench
+import md_simulation_cuda_b200 as mdb
 
 
 def _free_port():
@@ -29,7 +31,7 @@ def _worker(rank, world, port, out):
         from md_simulation_cuda_b200 import workloads as wl
 
         sizes = [len(f) for f, _ in wl.fire_mix(512)]
-        owner = bench.lpt_assign(sizes, world)
+        owner, _ = mdb.place_lpt(sizes, world)
         mine = [k for k, r in enumerate(owner) if r == rank]
         load = torch.tensor([float(sum(sizes[k] for k in mine))])
         loads = [torch.zeros(1) for _ in range(world)]
@@ -62,9 +64,33 @@ def test_two_cpu_ranks():
         assert not same_start and n == 4096  # replica seeds differ per rank
 
 
+def _lpt_reference(costs, nbins):
+    """Greedy LPT in Python: largest first (stable), least-loaded bin, ties low."""
+    order = sorted(range(len(costs)), key=lambda k: (-costs[k], k))
+    load = [0.0] * nbins
+    out = [0] * len(costs)
+    for k in order:
+        b = min(range(nbins), key=lambda d: (load[d], d))
+        out[k] = b
+        load[b] += costs[k]
+    return out, load
+
+
 def test_lpt_is_a_partition():
     costs = [5, 3, 3, 2, 2, 2, 1, 9]
-    owner = bench.lpt_assign(costs, 3)
-    assert sorted(set(owner)) == [0, 1, 2]
+    owner, load = mdb.place_lpt(costs, 3)
+    assert sorted(set(owner.tolist())) == [0, 1, 2]
     loads = [sum(c for c, o in zip(costs, owner) if o == b) for b in range(3)]
+    assert loads == load.tolist()
     assert sum(loads) == sum(costs) and max(loads) - min(loads) <= max(costs)
+
+
+def test_lpt_matches_the_rule_on_the_fire_mix():
+    from md_simulation_cuda_b200 import workloads as wl
+
+    costs = [len(f) * 20000.0 for f, _ in wl.fire_mix(512)]
+    for nb in (1, 2, 3, 8):
+        owner, load = mdb.place_lpt(costs, nb)
+        ref_owner, ref_load = _lpt_reference(costs, nb)
+        assert owner.tolist() == ref_owner and load.tolist() == ref_load
+        assert max(load) <= sum(costs) / nb + max(costs)
