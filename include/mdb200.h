@@ -334,10 +334,17 @@ int mdb_traj_writer_close(mdb_traj_writer_t* w);
  * step whose window mean and standard deviation are within tolerance_rel of
  * the target counts, stable_required such steps in a row end the warmup; it
  * ends anyway after warmup_max_steps) -> NPH_PRODUCTION (production_steps NPH
- * steps). Steps between two points where the protocol samples or decides run
- * as captured chunks; the decisions fall on the same steps as in the per-step
- * loop. records (up to cap) receive one entry per sample step, like the
- * driver's pressure log. */
+ * steps). The decisions fall on the same steps, with the same arithmetic, as
+ * in the driver's per-step loop. records (up to cap) receive one entry per
+ * sample step, like the driver's pressure log.
+ *
+ * By default the whole protocol is one graph launch: a while node runs one
+ * step per iteration, a switch node picks the Nose-Hoover or NPH step body,
+ * and the pressure samples, window statistics and phase switches are taken
+ * on the device; the host waits only after the last step. With host_driven
+ * set (or a handle created with use_graphs = 0) the host takes the decisions
+ * and issues the steps between two decision points as captured chunks,
+ * waiting once per sample. */
 typedef struct mdb_nph_protocol {
   int32_t auto_target;   /* 1: start with AUTO_TARGET ("auto_initial" mode)  */
   int32_t _pad0;
@@ -345,7 +352,8 @@ typedef struct mdb_nph_protocol {
   int32_t auto_steps, eval_interval, window_samples, stable_required;
   int32_t warmup_min_steps, warmup_max_steps, production_steps, _pad1;
   double tolerance_rel;
-  int32_t reserved[8];
+  int32_t host_driven;   /* 1: decisions on the host between step chunks      */
+  int32_t reserved[7];
 } mdb_nph_protocol_t;
 
 #define MDB_PHASE_AUTO_TARGET 0
@@ -369,6 +377,7 @@ typedef struct mdb_nph_result {
   int64_t n_records;       /* sample steps (may exceed cap)                 */
   int32_t forced_switch;   /* the warmup ended at warmup_max_steps          */
   int32_t finished;        /* production completed                          */
+  int64_t host_waits;      /* blocking waits of the host during the run     */
 } mdb_nph_result_t;
 
 /* The protocol parameters as the driver derives them from MDConfig

@@ -248,12 +248,17 @@ class MDSimulation:
         return out
 
     def run_nph_protocol(self, protocol: Optional[MDBNphProtocol] = None,
-                         record_cap: int = 100000):
+                         record_cap: int = 100000, host_driven: Optional[bool] = None):
         """The NPH driver protocol (AUTO_TARGET -> NPH_WARMUP -> NPH_PRODUCTION of
         tests/run_NPH_test/run_test_NPH.cpp); parameters from the config unless
-        given. Returns (result, records)."""
+        given. By default one graph launch with the decisions on the device;
+        host_driven=True takes them on the host between step chunks.
+        Returns (result, records)."""
         if protocol is None:
             protocol = nph_protocol_from_config(self.cfg_manager)
+        if host_driven is not None:
+            protocol = MDBNphProtocol.from_buffer_copy(protocol)
+            protocol.host_driven = 1 if host_driven else 0
         recs = (MDBNphRecord * max(1, record_cap))()
         res = MDBNphResult()
         check(lib().mdb_sim_run_nph_protocol(self._h, C.byref(protocol), recs, record_cap,

@@ -228,7 +228,8 @@ class MDBNphProtocol(C.Structure):
         ("window_samples", C.c_int32), ("stable_required", C.c_int32),
         ("warmup_min_steps", C.c_int32), ("warmup_max_steps", C.c_int32),
         ("production_steps", C.c_int32), ("_pad1", C.c_int32),
-        ("tolerance_rel", C.c_double), ("reserved", C.c_int32 * 8),
+        ("tolerance_rel", C.c_double), ("host_driven", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -246,6 +247,7 @@ class MDBNphResult(C.Structure):
         ("P_target", C.c_double), ("auto_end_step", C.c_int64),
         ("warmup_end_step", C.c_int64), ("total_steps", C.c_int64),
         ("n_records", C.c_int64), ("forced_switch", C.c_int32), ("finished", C.c_int32),
+        ("host_waits", C.c_int64),
     ]
 
 

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <memory>
 #include <new>
 #include <string>
@@ -101,6 +102,70 @@ int sim_export_async(mdb_sim_t* sim, mdb_particle_t* host, cudaEvent_t ev) {
 int64_t sim_particles(mdb_sim_t* sim) { return sim->eng->n(0); }
 
 int sim_device(mdb_sim_t* sim) { return sim->eng->device(); }
+
+long long sim_host_waits(mdb_sim_t* sim) { return sim->eng->host_waits(); }
+
+bool sim_uses_graphs(mdb_sim_t* sim) { return sim->eng->graphs(); }
+
+int sim_run_nph_protocol_graph(mdb_sim_t* sim, const mdb_nph_protocol_t& p,
+                               mdb_nph_record_t* rec, int64_t cap, mdb_nph_result_t* res) {
+  const long long waits0 = sim->eng->host_waits();
+  MDB_TRY(leave_piston(sim));
+  // parameters clamped as the host protocol clamps them
+  NphProto q;
+  memset(&q, 0, sizeof(q));
+  q.eval = std::max(1, p.eval_interval);
+  q.auto_steps = std::max(1, p.auto_steps);
+  q.window = std::max(2, p.window_samples);
+  q.stable_req = std::max(1, p.stable_required);
+  q.warm_min = std::max(0, p.warmup_min_steps);
+  q.warm_max = std::max<int64_t>(q.warm_min + 1, p.warmup_max_steps);
+  q.prod = std::max(1, p.production_steps);
+  q.hard = q.auto_steps + q.warm_max + q.prod + 50000;
+  q.tol = p.tolerance_rel;
+  q.W = sim->cfg.barostat_mass > 1e-12 ? sim->cfg.barostat_mass : 1e-12;
+  q.rate_init = sim->cfg.barostat_area_rate_init;
+  q.dt = sim->cfg.dt;
+  q.t = sim->t;
+  q.phase = p.auto_target ? 0 : 1;
+  q.P_target = p.auto_target ? 0.0 : p.P_target;
+  q.auto_end = -1;
+  q.warm_end = -1;
+  q.p_valid = sim->p_valid ? 1 : 0;
+  q.nph_init = sim->nph_init ? 1 : 0;
+  if (q.phase == 0) {
+    // the first Nose-Hoover step needs K of the current velocities
+    if (!sim->k_valid) MDB_TRY(sim->eng->reduce_K());
+  } else {
+    MDB_TRY(sim->eng->set_pext(q.P_target));
+  }
+  const int rc = sim->eng->run_nph_protocol(&q, rec, cap);
+  if (rc != MDB_OK) return rc;
+  sim->t = q.t;
+  sim->nph_init = q.nph_init != 0;
+  if (q.step > 0) {
+    if (q.last_phase == 0) {
+      sim->k_valid = true;
+      sim->p_valid = q.last_sample != 0;
+    } else {
+      sim->k_valid = false;
+      sim->p_valid = true;
+    }
+  }
+  memset(res, 0, sizeof(*res));
+  res->P_target = q.P_target;
+  res->auto_end_step = q.auto_end;
+  res->warmup_end_step = q.warm_end;
+  res->total_steps = q.step;
+  res->n_records = q.nrec;
+  res->forced_switch = q.forced;
+  res->finished = q.finished;
+  res->host_waits = sim->eng->host_waits() - waits0;
+  if (q.err == MDB_ERR_BOX && !q.nph_init)
+    return set_error(MDB_ERR_BOX, "invalid initial box for NPH");
+  if (q.err != 0) return check_status(sim);
+  return MDB_OK;
+}
 
 }  // namespace mdb
 

@@ -19,8 +19,6 @@
 
 namespace mdb {
 
-namespace {
-
 void* force_fn(int fm, bool py) {
 #define MDB_F(M) return py ? (void*)k_force<M, true> : (void*)k_force<M, false>
   switch (fm) {
@@ -44,6 +42,8 @@ void* drift_fn(int dm) {
     default: return (void*)k_drift<DM_FIRE>;
   }
 }
+
+namespace {
 
 double next_pow2(double x) {
   double b = 1.0;
@@ -69,7 +69,7 @@ Engine::Engine(const mdb_options_t& opt) {
 
 Engine::~Engine() {
   cudaSetDevice(device_);
-  if (stream_) cudaStreamSynchronize(stream_);
+  if (stream_) cudaStreamSynchronize(stream_);  // destructor: not counted
   drop_graphs();
   for (void* p : allocs_) cudaFree(p);
   if (stream_) cudaStreamDestroy(stream_);
@@ -378,7 +378,7 @@ int Engine::build() {
   MDB_CUDA(cudaMemsetAsync(D.part, 0, sizeof(double) * (size_t)nblocks_ * kNP, stream_));
   MDB_CUDA(cudaMemsetAsync(D.partm, 0, sizeof(double) * (size_t)nblocks_ * 4, stream_));
   MDB_CUDA(cudaMemsetAsync(D.cell_of, 0, sizeof(int32_t) * (size_t)ntot_, stream_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   built_ = true;
   for (int s = 0; s < ns; ++s) {
     rc = set_frame(s, specs_[s].frame.data());
@@ -668,7 +668,7 @@ int Engine::run_fire(int64_t iters) {
 int Engine::get_state(int s, SysState* out) {
   MDB_CUDA(cudaSetDevice(device_));
   MDB_CUDA(cudaMemcpyAsync(out, dev_.st + s, sizeof(SysState), cudaMemcpyDeviceToHost, stream_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   return MDB_OK;
 }
 
@@ -677,14 +677,14 @@ int Engine::get_states(std::vector<SysState>& out) {
   out.resize(specs_.size());
   MDB_CUDA(cudaMemcpyAsync(out.data(), dev_.st, sizeof(SysState) * out.size(),
                            cudaMemcpyDeviceToHost, stream_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   return MDB_OK;
 }
 
 int Engine::put_state(int s, const SysState& st) {
   MDB_CUDA(cudaSetDevice(device_));
   MDB_CUDA(cudaMemcpyAsync(dev_.st + s, &st, sizeof(SysState), cudaMemcpyHostToDevice, stream_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   return MDB_OK;
 }
 
@@ -698,7 +698,7 @@ int Engine::get_frame(int s, mdb_particle_t* out) {
   count_launches(1);
   MDB_CUDA(cudaMemcpyAsync(out, d_aos_, sizeof(mdb_particle_t) * (size_t)P.n,
                            cudaMemcpyDeviceToHost, stream_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   return MDB_OK;
 }
 
@@ -731,7 +731,7 @@ int Engine::profiles(int s, int nb, bool py, double* ptens, int32_t* counts) {
   if (e == cudaSuccess && counts)
     e = cudaMemcpyAsync(counts, d_cnt, sizeof(int) * 2 * (size_t)nb, cudaMemcpyDeviceToHost,
                         stream_);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e == cudaSuccess) e = wait_host();
   cudaFree(d_acc);
   cudaFree(d_cnt);
   if (e != cudaSuccess) return cuda_error(e, "profiles");
@@ -784,13 +784,13 @@ int Engine::debug_cells(int s, int32_t* orig, int32_t* cell) {
                            cudaMemcpyDeviceToHost, stream_));
   MDB_CUDA(cudaMemcpyAsync(cell, dev_.cell_of + P.p0, sizeof(int32_t) * (size_t)P.n,
                            cudaMemcpyDeviceToHost, stream_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   return MDB_OK;
 }
 
 int Engine::sync() {
   MDB_CUDA(cudaSetDevice(device_));
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   return MDB_OK;
 }
 
@@ -962,7 +962,7 @@ int Engine::tune() {
                              cudaMemcpyDeviceToDevice, stream_));
     MDB_CUDA(cudaMemcpyAsync(dev_.st, snap.data(), sizeof(SysState) * snap.size(),
                              cudaMemcpyHostToDevice, stream_));
-    MDB_CUDA(cudaStreamSynchronize(stream_));
+    MDB_CUDA(wait_host());
     // rebuild: list-build grid, then the grid of the other rebuild kernels
     const int one_wave = nlist_grid_;
     const int64_t work = std::max(ntot_, ncells_);
@@ -997,7 +997,7 @@ int Engine::tune() {
     dev_.rb_grid = rb_grid_;
     cache_store(key, dev_.pf_rows, nlist_grid_, rb_grid_);
   }
-  MDB_CUDA(cudaStreamSynchronize(stream_));
+  MDB_CUDA(wait_host());
   schedule_.list_prefetch_rows = dev_.pf_rows;
   schedule_.nlist_grid = nlist_grid_;
   schedule_.rebuild_grid = rb_grid_;

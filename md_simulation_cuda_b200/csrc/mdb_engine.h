@@ -88,6 +88,19 @@ class Engine {
   // Kernel launches issued (eager launches + kernel nodes of launched graphs,
   // counting the rebuild body once per rebuild actually run).
   long long launches_issued() const { return launches_; }
+  // Times the host has blocked on the engine's stream (state and frame reads,
+  // sync()); the destructor's final wait is not counted.
+  long long host_waits() const { return host_waits_; }
+
+  // The NPH driver protocol of a single system in one graph launch. A while
+  // node runs one step per iteration; a switch node picks the Nose-Hoover
+  // body, the NPH body, or the NPH body preceded by the NPH entry (pressure
+  // observation and barostat initialisation); a one-thread kernel takes the
+  // protocol's decisions on the device after each step and writes the
+  // records. q holds the parameters and the initial loop state on entry and
+  // the final loop state on return; rec receives min(q->nrec, cap) records.
+  // The host waits twice, both after the last step.
+  int run_nph_protocol(NphProto* q, mdb_nph_record_t* rec, int64_t cap);
 
  private:
   int ensure_device();
@@ -106,6 +119,10 @@ class Engine {
   int time_force(int fm, int reps, double* ms);
   int time_rebuild(int reps, double* ms);
   void drop_graphs();
+  cudaError_t wait_host() {
+    ++host_waits_;
+    return cudaStreamSynchronize(stream_);
+  }
 
   int device_ = 0;
   double skin_ = 0.0;
@@ -120,20 +137,25 @@ class Engine {
   int nblocks_ = 0;
   int rb_grid_ = 0;
   int scan_grid_ = 0;
-  int nlist_grid_ = 0;
+  int nlist_grid_ = 0;  // k_rb_nlist: one wave of resident blocks
   int fire_prec_ = MDB_FIRE_AUTO;
   int autotune_ = 0;
   mdb_schedule_t schedule_{};
-  int stream_priority_ = 0;  // levels above normal for stream_  // k_rb_nlist: one wave of resident blocks
+  int stream_priority_ = 0;  // levels above normal for stream_
   int64_t aos_cap_ = 0;
   void* d_aos_ = nullptr;
   void* d_obs_ = nullptr;  // one mdb_observables_t staging slot
   std::vector<void*> allocs_;
   std::map<std::tuple<int, int, int, int, int>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
   long long launches_ = 0;
+  long long host_waits_ = 0;
   int64_t bytes_ = 0;
   long long last_rebuilds_ = 0;
 };
+
+// Kernel of a force phase (FM_*; py: periodic y) and of a drift phase (DM_*).
+void* force_fn(int fm, bool py);
+void* drift_fn(int dm);
 
 int reference_initial_frame(const mdb_config_t& cfg, std::vector<mdb_particle_t>& out);
 
@@ -142,5 +164,13 @@ int reference_initial_frame(const mdb_config_t& cfg, std::vector<mdb_particle_t>
 int sim_export_async(mdb_sim_t* sim, mdb_particle_t* host, cudaEvent_t ev);
 int64_t sim_particles(mdb_sim_t* sim);
 int sim_device(mdb_sim_t* sim);
+// The NPH driver protocol of a simulation in one graph launch (the decisions
+// on the device); host_waits receives the host's blocking waits it took.
+int sim_run_nph_protocol_graph(mdb_sim_t* sim, const mdb_nph_protocol_t& p,
+                               mdb_nph_record_t* rec, int64_t cap, mdb_nph_result_t* res);
+// Blocking waits of the host on the simulation's stream so far.
+long long sim_host_waits(mdb_sim_t* sim);
+// Whether the simulation issues its steps as CUDA graphs.
+bool sim_uses_graphs(mdb_sim_t* sim);
 
 }  // namespace mdb

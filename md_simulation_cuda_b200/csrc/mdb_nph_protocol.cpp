@@ -6,11 +6,14 @@
 // step limit) -> NPH_PRODUCTION (a fixed number of NPH steps).
 //
 // The reference runs one step per loop iteration with a host round trip each
-// time. Here the steps between two points where the protocol can observe or
+// time. By default the whole protocol runs as one graph launch with the
+// decisions on the device (mdb_nph_graph.cu). The host-driven form here
+// issues the steps between two points where the protocol can observe or
 // decide anything (a pressure sample, the end of a phase, the step at which
-// the warmup criterion can first be met) are issued as one chunk of captured
-// steps, so the host waits once per sample instead of once per step. The
-// decisions are taken exactly where the per-step loop takes them.
+// the warmup criterion can first be met) as one chunk of captured steps, so
+// the host waits once per sample instead of once per step; it also serves the
+// dry run. The decisions are taken exactly where the per-step loop takes
+// them.
 #include <math.h>
 #include <string.h>
 
@@ -20,6 +23,7 @@
 #include <vector>
 
 #include "mdb200.h"
+#include "mdb_engine.h"
 #include "mdb_util.h"
 
 namespace {
@@ -261,9 +265,15 @@ int mdb_nph_protocol_from_config(const mdb_config_t* cfg, mdb_nph_protocol_t* ou
 
 int mdb_sim_run_nph_protocol(mdb_sim_t* sim, const mdb_nph_protocol_t* protocol,
                              mdb_nph_record_t* records, int64_t cap, mdb_nph_result_t* result) {
-  if (!sim || !protocol || !result || cap < 0) return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (!sim || !protocol || !result || cap < 0 || (cap > 0 && !records))
+    return mdb::set_error(MDB_ERR_ARG, "bad arguments");
+  if (!protocol->host_driven && mdb::sim_uses_graphs(sim))
+    return mdb::sim_run_nph_protocol_graph(sim, *protocol, records, cap, result);
+  const long long waits0 = mdb::sim_host_waits(sim);
   SimDriver d(sim);
-  return run_protocol(d, *protocol, records, cap, result);
+  const int rc = run_protocol(d, *protocol, records, cap, result);
+  result->host_waits = mdb::sim_host_waits(sim) - waits0;
+  return rc;
 }
 
 int mdb_nph_protocol_dry_run(const mdb_nph_protocol_t* protocol, const double* pressures,

@@ -63,6 +63,22 @@ def test_noalloc_matches_compute_forces_two_calls(built):
     assert first[1] == again[1] and first[2] == again[2]
 
 
+def test_noalloc_against_fp64_oracle(built):
+    """The entry point checked on its own: accelerations, U and W against the
+    FP64 oracle, periodic and walled in y."""
+    from oracle import pyoracle as po
+
+    f, cfg = wl.nve_4096(seed=11)
+    Lx, Ly = cfg["box_w_global"], cfg["box_h_global"]
+    for periodic_y in (True, False):
+        a, u, w = _noalloc(cfg, f, Lx, Ly, periodic_y)
+        ref, U0, W0 = po.forces(cfg, f["pos"], f["type"], Lx, Ly, mode=po.OR_FP64,
+                                periodic_y=1 if periodic_y else 0)
+        assert rel_l2(a, ref) <= FORCE_TOL
+        assert rel_err(u, U0) <= 1e-6
+        assert rel_err(w, W0) <= 1e-6
+
+
 def test_noalloc_walls_small_box_and_other_types(built):
     f, Lx, Ly = wl.lattice_frame(3000, 0.8, 2.0, 0.65, 1.0, seed=9)
     cfg = wl.config_dict(3000, Lx, Ly, dt=0.001)
