@@ -71,6 +71,7 @@ Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);  // destructor: not counted
   drop_graphs();
+  free_proto();
   for (void* p : allocs_) cudaFree(p);
   if (stream_) cudaStreamDestroy(stream_);
 }

@@ -97,9 +97,10 @@ class Engine {
   // body, the NPH body, or the NPH body preceded by the NPH entry (pressure
   // observation and barostat initialisation); a one-thread kernel takes the
   // protocol's decisions on the device after each step and writes the
-  // records. q holds the parameters and the initial loop state on entry and
-  // the final loop state on return; rec receives min(q->nrec, cap) records.
-  // The host waits twice, both after the last step.
+  // records; steps between two decision points run as quiet chunks of 64, 8
+  // or 1 steps. q holds the parameters and the initial loop state on entry
+  // and the final loop state on return; rec receives min(q->nrec, cap)
+  // records. The host waits at most twice, both after the last step.
   int run_nph_protocol(NphProto* q, mdb_nph_record_t* rec, int64_t cap);
 
  private:
@@ -119,6 +120,9 @@ class Engine {
   int time_force(int fm, int reps, double* ms);
   int time_rebuild(int reps, double* ms);
   void drop_graphs();
+  // The cached protocol graph (built at the first protocol run).
+  int proto_graph(cudaGraphExec_t* exec);
+  void free_proto();
   cudaError_t wait_host() {
     ++host_waits_;
     return cudaStreamSynchronize(stream_);
@@ -149,6 +153,10 @@ class Engine {
   std::map<std::tuple<int, int, int, int, int>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
   long long launches_ = 0;
   long long host_waits_ = 0;
+  NphProto* d_proto_ = nullptr;  // protocol loop state (address baked into its graph)
+  double* proto_win_ = nullptr;
+  void* proto_rec_ = nullptr;
+  int64_t proto_win_cap_ = 0, proto_rec_cap_ = 0;
   int64_t bytes_ = 0;
   long long last_rebuilds_ = 0;
 };

@@ -112,21 +112,29 @@ struct BatchGlobal {
 
 // The NPH driver protocol (run_test_NPH.cpp:137-290) run on the device: its
 // parameters, clamped as the host protocol clamps them, and the loop state,
-// advanced once per step by a one-thread kernel inside a graph while loop.
+// advanced by a one-thread kernel after each iteration of a graph while loop
+// (one decision step, a chunk of quiet steps, or the NPH entry).
 struct NphProto {
   int64_t eval, auto_steps, window, stable_req, warm_min, warm_max, prod, hard, cap;
   double tol;
   double W, rate_init;  // barostat mass (>= 1e-12) and initial area rate
   double dt;            // time added per step (advance_time)
+  double* win;          // window ring, `window` slots
+  void* rec;            // mdb_nph_record_t[cap]
   double P_target, auto_sum, t;
   int64_t step, auto_done, warm_done, prod_done, stable, auto_n, nrec;
   int64_t auto_end, warm_end;
   int64_t win_n, win_head;  // samples in the window ring, slot of the oldest
+  int64_t iters;            // while-loop iterations run
   int32_t phase;            // phase of the next step
   int32_t p_valid;          // S.P_cur holds the pressure of the current state
   int32_t nph_init;         // NPH area momentum and aspect initialised
   int32_t forced, finished, err;
   int32_t last_phase, last_sample;  // phase of the last step, whether it was sampled
+  int32_t pending;          // what the body of the running iteration does
+  int32_t pending_steps;    // its steps (quiet chunks)
+  int32_t window_ok;        // stability test of the current window (quiet chunks)
+  int32_t pad;
 };
 
 // Kernel argument block (passed by value).
