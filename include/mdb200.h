@@ -132,8 +132,22 @@ typedef struct mdb_options {
                              ~/.cache/md_simulation_cuda_b200/schedule.txt).
                              None of these changes any result bit.
                              0 (default): the built-in schedule           */
-  int32_t reserved[9];
+  int32_t step_kernel;    /* MD steps of a single-system handle:
+                             MDB_STEPS_AUTO (0, default): the multi-step
+                             kernel when every block of the system fits on
+                             the device at once (one cooperative launch runs
+                             the drift and force phases of many steps, with
+                             grid barriers between them) and the system is
+                             small enough that launches dominate a step;
+                             MDB_STEPS_PER_PHASE: one kernel per phase;
+                             MDB_STEPS_MULTI: the multi-step kernel whenever
+                             it fits. Both give the same result bits.       */
+  int32_t reserved[8];
 } mdb_options_t;
+
+#define MDB_STEPS_AUTO 0
+#define MDB_STEPS_PER_PHASE 1
+#define MDB_STEPS_MULTI 2
 
 #define MDB_FIRE_AUTO 0
 #define MDB_FIRE_FP32 1
@@ -151,6 +165,8 @@ typedef struct mdb_schedule {
   int32_t from_cache;         /* 1: read from the schedule cache file        */
   double skin;                /* neighbour-list skin                         */
   double tune_ms;             /* time spent timing candidates                */
+  int32_t multi_step;         /* 1: MD steps run in the multi-step kernel    */
+  int32_t multi_step_blocks;  /* blocks the device holds at once for it      */
 } mdb_schedule_t;
 
 /* MDConfig{} value-initialised defaults (include/md_config.hpp:14-75). */

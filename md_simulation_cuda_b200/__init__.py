@@ -26,7 +26,8 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import (FIRE_AUTO, FIRE_FP32, FIRE_FP64, MDB_ERR_ARG, MDBConfigC, MDBError,
+from ._lib import (FIRE_AUTO, FIRE_FP32, FIRE_FP64, STEPS_AUTO, STEPS_MULTI, STEPS_PER_PHASE,
+                   MDB_ERR_ARG, MDBConfigC, MDBError,
                    MDBFireParams, MDBMinimizeResult,
                    MDBNphProtocol, MDBNphRecord, MDBNphResult, MDBObservables, MDBRequest,
                    MDBRequestResult, MDBServerOptions, MDBServerStats, PARTICLE_DTYPE, check,
@@ -155,11 +156,12 @@ class MDSimulation:
                  step: Optional[int] = None, *, frame=None, device: int = 0,
                  skin: Optional[float] = None, use_graphs: bool = True,
                  state_file: Optional[str] = None, max_neighbors: Optional[int] = None,
-                 autotune: bool = False):
+                 autotune: bool = False, step_kernel: Optional[int] = None):
         self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
             else MDConfigManager(_config_of(config_manager))
         self._h = C.c_void_p()
-        opt = options(device, skin, use_graphs, max_neighbors, autotune=autotune)
+        opt = options(device, skin, use_graphs, max_neighbors, autotune=autotune,
+                      step_kernel=step_kernel)
         cfg = self.cfg_manager.config
         if state_file is not None:
             # a checkpoint: frame `step` of `filename` plus the integrator state

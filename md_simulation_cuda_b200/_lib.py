@@ -102,7 +102,8 @@ class MDBOptions(C.Structure):
         ("stream_priority", C.c_int32),
         ("fire_precision", C.c_int32),
         ("autotune", C.c_int32),
-        ("reserved", C.c_int32 * 9),
+        ("step_kernel", C.c_int32),
+        ("reserved", C.c_int32 * 8),
     ]
 
 
@@ -116,6 +117,8 @@ class MDBSchedule(C.Structure):
         ("from_cache", C.c_int32),
         ("skin", C.c_double),
         ("tune_ms", C.c_double),
+        ("multi_step", C.c_int32),
+        ("multi_step_blocks", C.c_int32),
     ]
 
     def as_dict(self):
@@ -398,13 +401,16 @@ def check(rc: int):
 
 
 FIRE_AUTO, FIRE_FP32, FIRE_FP64 = 0, 1, 2
+STEPS_AUTO, STEPS_PER_PHASE, STEPS_MULTI = 0, 1, 2
 
 
 def options(device=0, skin=None, use_graphs=True, max_neighbors=None,
-            fire_precision=None, autotune=None) -> MDBOptions:
+            fire_precision=None, autotune=None, step_kernel=None) -> MDBOptions:
     o = MDBOptions()
     lib().mdb_options_default(C.byref(o))
     o.device = device
+    if step_kernel is not None:
+        o.step_kernel = int(step_kernel)
     if autotune is not None:
         o.autotune = 1 if autotune else 0
     if fire_precision is not None:

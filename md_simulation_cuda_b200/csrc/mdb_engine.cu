@@ -43,6 +43,14 @@ void* drift_fn(int dm) {
   }
 }
 
+void* steps_fn(int dm) {
+  switch (dm) {
+    case DM_NVE: return (void*)k_md_steps<DM_NVE, FM_NVE>;
+    case DM_NH: return (void*)k_md_steps<DM_NH, FM_NH>;
+    default: return (void*)k_md_steps<DM_NPH, FM_NPH>;
+  }
+}
+
 namespace {
 
 double next_pow2(double x) {
@@ -61,6 +69,7 @@ Engine::Engine(const mdb_options_t& opt) {
   stream_priority_ = opt.stream_priority > 0 ? opt.stream_priority : 0;
   fire_prec_ = opt.fire_precision;
   autotune_ = opt.autotune;
+  step_kernel_ = opt.step_kernel;
   // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
   // see kernel nodes of graphs that contain conditional nodes).
   const char* eager = getenv("MDB_EAGER");
@@ -400,7 +409,133 @@ int Engine::build() {
   schedule_.rebuild_grid = rb_grid_;
   schedule_.items = items_max;
   schedule_.skin = skin_;
+  rc = choose_multi_step();
+  if (rc) return rc;
   return autotune_ ? tune() : MDB_OK;
+}
+
+// The multi-step kernel needs every block of the (single) system resident at
+// once. AUTO takes it for systems of at most kMultiStepMaxBlocks blocks, where
+// the per-phase launches and their tails dominate a step.
+int Engine::choose_multi_step() {
+  multi_step_ = false;
+  multi_cap_ = 0;
+  schedule_.multi_step = 0;
+  schedule_.multi_step_blocks = 0;
+  if (nsys() != 1 || !use_graphs_ || step_kernel_ == MDB_STEPS_PER_PHASE) return MDB_OK;
+  int nsm = 0;
+  MDB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_));
+  int coop = 0;
+  MDB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device_));
+  if (!coop) return MDB_OK;
+  int per_sm = 1 << 30;
+  for (int dm : {DM_NVE, DM_NH, DM_NPH}) {
+    int b = 0;
+    MDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, steps_fn(dm), kThreads, 0));
+    per_sm = std::min(per_sm, b);
+  }
+  multi_cap_ = per_sm * nsm;
+  const bool fits = nblocks_ >= 1 && nblocks_ <= multi_cap_;
+  if (step_kernel_ == MDB_STEPS_MULTI)
+    multi_step_ = fits;
+  else
+    multi_step_ = fits && nblocks_ <= kMultiStepMaxBlocks;
+  schedule_.multi_step = multi_step_ ? 1 : 0;
+  schedule_.multi_step_blocks = multi_cap_;
+  return MDB_OK;
+}
+
+// while (more) { k_md_steps ; if (rebuild) { rebuild ; force ; count } }
+int Engine::get_steps_graph(int dm, int fm, cudaGraphExec_t* exec) {
+  auto key = std::make_tuple(3, dm, fm, 1, 0);
+  auto it = graphs_.find(key);
+  if (it != graphs_.end()) {
+    *exec = it->second.second;
+    return MDB_OK;
+  }
+  cudaGraph_t g;
+  MDB_CUDA(cudaGraphCreate(&g, 0));
+  int rc = MDB_OK;
+  auto ck = [&](cudaError_t e, const char* what) {
+    if (rc == MDB_OK && e != cudaSuccess) rc = cuda_error(e, what);
+    return rc == MDB_OK;
+  };
+  cudaGraphConditionalHandle h_more = 0, h_rb = 0;
+  ck(cudaGraphConditionalHandleCreate(&h_more, g, 1, cudaGraphCondAssignDefault), "handle");
+  ck(cudaGraphConditionalHandleCreate(&h_rb, g, 0, 0), "handle");
+  cudaGraph_t body = nullptr, rb_body = nullptr;
+  cudaGraphNode_t nwhile, nsteps, nif;
+  if (rc == MDB_OK) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_more;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (ck(cudaGraphAddNode(&nwhile, g, nullptr, 0, &cp), "cudaGraphAddNode(while)"))
+      body = cp.conditional.phGraph_out[0];
+  }
+  Dev d = dev_;
+  d.use_cond = 0;
+  if (rc == MDB_OK) {
+    void* args[] = {&d, &h_more, &h_rb};
+    cudaKernelNodeParams kp = {};
+    kp.func = steps_fn(dm);
+    kp.gridDim = dim3(nblocks_);
+    kp.blockDim = dim3(kThreads);
+    kp.kernelParams = args;
+    if (ck(cudaGraphAddKernelNode(&nsteps, body, nullptr, 0, &kp), "cudaGraphAddKernelNode")) {
+      cudaLaunchAttributeValue v = {};
+      v.cooperative = 1;
+      ck(cudaGraphKernelNodeSetAttribute(nsteps, cudaLaunchAttributeCooperative, &v),
+         "cudaGraphKernelNodeSetAttribute(cooperative)");
+    }
+  }
+  if (rc == MDB_OK) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_rb;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    if (ck(cudaGraphAddNode(&nif, body, &nsteps, 1, &cp), "cudaGraphAddNode(if)"))
+      rb_body = cp.conditional.phGraph_out[0];
+  }
+  if (rc == MDB_OK) rc = add_rebuild_body(rb_body, d);
+  if (rc == MDB_OK) {
+    // the rebuild body ends in its one finish kernel: the force phase of the
+    // pending step and the count follow it
+    size_t nn = 0;
+    ck(cudaGraphGetNodes(rb_body, nullptr, &nn), "cudaGraphGetNodes");
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (rc == MDB_OK) ck(cudaGraphGetNodes(rb_body, nodes.data(), &nn), "cudaGraphGetNodes");
+    cudaGraphNode_t last = nullptr;
+    for (size_t k = 0; k < nn && rc == MDB_OK; ++k) {
+      size_t nd = 0;
+      ck(cudaGraphNodeGetDependentNodes(nodes[k], nullptr, &nd), "cudaGraphNodeGetDependentNodes");
+      if (nd == 0) last = nodes[k];
+    }
+    if (rc == MDB_OK && !last) rc = set_error(MDB_ERR_STATE, "rebuild body has no last node");
+    cudaGraphNode_t nf, nc;
+    if (rc == MDB_OK)
+      rc = add_kernel_node(rb_body, &last, 1, force_fn(fm, true), nblocks_, kThreads, dev_, &nf);
+    if (rc == MDB_OK) {
+      void* args[] = {&d, &h_more};
+      cudaKernelNodeParams kp = {};
+      kp.func = (void*)k_md_steps_count;
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(32);
+      kp.kernelParams = args;
+      ck(cudaGraphAddKernelNode(&nc, rb_body, &nf, 1, &kp), "cudaGraphAddKernelNode");
+    }
+  }
+  cudaGraphExec_t ex = nullptr;
+  if (rc == MDB_OK) ck(cudaGraphInstantiate(&ex, g, 0), "cudaGraphInstantiate(steps)");
+  if (rc != MDB_OK) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  graphs_[key] = std::make_pair(g, ex);
+  *exec = ex;
+  return MDB_OK;
 }
 
 int Engine::launch(void* fn, int grid, int block, const Dev& d) {
@@ -576,6 +711,18 @@ int Engine::get_graph(int kind, int dm, int fm, bool py, int chunk, cudaGraphExe
 int Engine::run_md(int dm, int fm, bool py, int64_t nsteps) {
   if (!built_) return set_error(MDB_ERR_STATE, "engine not built");
   MDB_CUDA(cudaSetDevice(device_));
+  if (multi_step_ && py && nsteps > 0 && (dm == DM_NVE || dm == DM_NH || dm == DM_NPH)) {
+    cudaGraphExec_t ex;
+    const int grc = get_steps_graph(dm, fm, &ex);
+    if (grc != MDB_OK) return grc;
+    k_md_steps_set<<<1, 32, 0, stream_>>>(dev_, nsteps);
+    MDB_CUDA(cudaGetLastError());
+    MDB_CUDA(cudaGraphLaunch(ex, stream_));
+    // the count kernel and one multi-step launch (more after each rebuild)
+    launches_ += 2;
+    count_launches(2);
+    return MDB_OK;
+  }
   int64_t left = nsteps;
   if (use_graphs_) {
     static const int kChunks[] = {64, 8, 1};

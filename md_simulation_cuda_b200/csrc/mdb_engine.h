@@ -122,6 +122,10 @@ class Engine {
   void drop_graphs();
   // The cached protocol graph (built at the first protocol run).
   int proto_graph(cudaGraphExec_t* exec);
+  // Whether MD steps run in the multi-step kernel (single system, all
+  // blocks resident), and its cached graph per drift/force mode.
+  int choose_multi_step();
+  int get_steps_graph(int dm, int fm, cudaGraphExec_t* exec);
   void free_proto();
   cudaError_t wait_host() {
     ++host_waits_;
@@ -144,6 +148,9 @@ class Engine {
   int nlist_grid_ = 0;  // k_rb_nlist: one wave of resident blocks
   int fire_prec_ = MDB_FIRE_AUTO;
   int autotune_ = 0;
+  int step_kernel_ = MDB_STEPS_AUTO;
+  bool multi_step_ = false;
+  int multi_cap_ = 0;  // blocks of the multi-step kernel the device holds at once
   mdb_schedule_t schedule_{};
   int stream_priority_ = 0;  // levels above normal for stream_
   int64_t aos_cap_ = 0;

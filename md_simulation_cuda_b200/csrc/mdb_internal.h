@@ -34,6 +34,9 @@ constexpr int32_t kListInterior = 1 << 30;
 // Force phase: list rows of the next chunk prefetched into L1 per warp
 // (built-in schedule; Dev::pf_rows holds the one in use).
 constexpr int kListPrefetchRows = 28;
+// MD steps of a single system of at most this many blocks run in the
+// multi-step kernel by default (MDB_STEPS_AUTO).
+constexpr int kMultiStepMaxBlocks = 148;
 
 // Force-phase variants.
 enum FMode : int32_t {
@@ -108,6 +111,11 @@ struct BatchGlobal {
   uint32_t sys_counter;
   int32_t nsys;
   int32_t all_done;
+  int64_t steps_left;  // multi-step kernel: steps of the running call not yet done
+  uint32_t bar_count;  // multi-step kernel: grid barrier arrivals
+  uint32_t bar_gen;    //   and generation
+  int32_t bar_err;     //   a barrier wait ran out of polls
+  int32_t pad;
 };
 
 // The NPH driver protocol (run_test_NPH.cpp:137-290) run on the device: its

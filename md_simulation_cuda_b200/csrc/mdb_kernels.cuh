@@ -397,7 +397,21 @@ __device__ __forceinline__ void pair_one(const float4 q, const PairCtx& c, float
 // else int32 at nlist[k * ntot + i]. MIC = false is the interior form: no
 // minimum image and no offset wrap (j = i + d). Offsets are fetched several at
 // a time before the dependent position gathers to keep loads in flight.
-template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, bool FLOOR, typename IDX>
+// Position loads of the pair loop. NC: through the read-only data path, for
+// kernels that do not write positions. Otherwise a plain (weak, L1-cached)
+// load: the multi-step kernel writes the positions between its phases, and
+// the acquire of its grid barrier makes those writes visible to it.
+template <bool NC>
+__device__ __forceinline__ float4 ld_pos(const float4* p) {
+  if (NC) return __ldg(p);
+  float4 v;
+  asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p));
+  return v;
+}
+
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, bool FLOOR, bool NC, typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
                                           int li, int n, int nn, const PairCtx& c, float2& fs,
@@ -422,7 +436,7 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
     }
 #pragma unroll
     for (int q = 0; q < PF; ++q)
-      pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + j[q]), c, fs, fc, ws, wc, u, an);
+      pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(ld_pos<NC>(base + j[q]), c, fs, fc, ws, wc, u, an);
   }
   for (; k < nn; ++k) {
     int t = (int)__ldg(p + (int64_t)k * ntot);
@@ -431,18 +445,18 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
       t += (t < 0) ? n : 0;
       t -= (t >= n) ? n : 0;
     }
-    pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(__ldg(base + t), c, fs, fc, ws, wc, u, an);
+    pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(ld_pos<NC>(base + t), c, fs, fc, ws, wc, u, an);
   }
 }
 
 // Candidates j in [j0, j1) (cell stencil rows or the whole system).
-template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR>
+template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR, bool NC>
 __device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
                                            const PairCtx& c, float2& fs, float2& fc, float& ws,
                                            float& wc, double& u, double& an) {
 #pragma unroll 4
   for (int j = j0; j < j1; ++j)
-    pair_one<PY, ENERGY, VIRIAL, true, FLOOR>(__ldg(pff + j), c, fs, fc, ws, wc, u, an);
+    pair_one<PY, ENERGY, VIRIAL, true, FLOOR>(ld_pos<NC>(pff + j), c, fs, fc, ws, wc, u, an);
 }
 
 __device__ __forceinline__ void split_box(double L, float& h, float& l, float& inv) {
@@ -485,13 +499,13 @@ __device__ __forceinline__ void set_profile_class(PairCtx& c, const SysParams& P
 // system for grids narrower than 3 cells). Returns F in FP64. tci receives the
 // type class of slot i, decoded from its float-float position (encode_ff), so
 // the type array is not read.
-template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR = false>
+template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR = false, bool NC = true>
 __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
                                                int64_t i, double Lx, double Ly, double& fx,
                                                double& fy, double& w, double& u, double& an,
                                                int& tci) {
   PairCtx c;
-  const float4 qi = __ldg(D.pff + i);
+  const float4 qi = ld_pos<NC>(D.pff + i);
   set_pair_box<PY>(c, qi, Lx, Ly);
   tci = (int)ff_class(qi);
   c.ts = (tci == 2) ? 99u : (uint32_t)tci;
@@ -524,21 +538,21 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
     const int nn = nc & (kListInterior - 1);
     if (D.nl16) {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR, NC>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
                                                   wc, u, an);
       else
-        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR, NC>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
                                                  wc, u, an);
     } else {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR, NC>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
                                                   wc, u, an);
       else
-        pair_list<PY, ENERGY, VIRIAL, true, FLOOR>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR, NC>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
                                                  wc, u, an);
     }
   } else if (S.allpairs) {
-    pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fs, fc, ws, wc,
+    pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fs, fc, ws, wc,
                                           u, an);
   } else {
     const int ncx = S.ncx, ncy = S.ncy;
@@ -556,17 +570,17 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
       }
       const int64_t row = P.c0 + (int64_t)yy * ncx;
       if (cx > 0 && cx < ncx - 1) {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + cx - 1),
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row + cx - 1),
                                               __ldg(cs + row + cx + 2), c, fs, fc, ws, wc, u, an);
       } else if (cx == 0) {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fs, fc,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fs, fc,
                                               ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 1),
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row + ncx - 1),
                                               __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an);
       } else {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row + ncx - 2),
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row + ncx - 2),
                                               __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL, FLOOR>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fs, fc,
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fs, fc,
                                               ws, wc, u, an);
       }
     }
@@ -865,9 +879,12 @@ __device__ __noinline__ ForceFinish<FM, PY> force_items_hp(Dev D, const SysParam
 // One thread per slot. FM selects what follows the force evaluation; PY is the
 // y image convention (false = the piston's walled y axis, which also applies
 // the soft walls in FM_INIT/FM_OBS).
-template <int FM, bool PY>
-__global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
-  const int b = blockIdx.x;
+//
+// force_phase is the work of block b of the launch; k_force runs it as one
+// kernel, k_md_steps as a phase of its multi-step loop (NC = false: plain
+// position loads, see ld_pos).
+template <int FM, bool PY, bool NC>
+__device__ __forceinline__ void force_phase(const Dev& D, const int b) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
@@ -945,7 +962,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
       double fx, fy, w, u, an;
       int tci;
       if (i < end) {
-        particle_force<PY, kEnergy, kVirial, kHpCapable>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an,
+        particle_force<PY, kEnergy, kVirial, kHpCapable, NC>(D, P, *S, i, Lx, Ly, fx, fy, w, u, an,
                                                          tci);
         fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
       }
@@ -1041,6 +1058,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
   S->counter = 0u;
 }
 
+template <int FM, bool PY>
+__global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
+  force_phase<FM, PY, true>(D, blockIdx.x);
+}
+
 // ------------------------------------------------------------ drift phase --
 // First half of a step for one slot: kick + drift + wrap (mode-specific),
 // float-float refresh, displacement since the last rebuild. The system's last
@@ -1127,9 +1149,10 @@ __device__ __forceinline__ void drift_particle(const Dev& D, const DriftCtx& c, 
   }
 }
 
+// drift_phase is the work of block b of the launch (k_drift: one kernel;
+// k_md_steps: a phase of its multi-step loop).
 template <int DMd>
-__global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
-  const int b = blockIdx.x;
+__device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
@@ -1298,6 +1321,112 @@ __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
   }
   S->counter = 0u;
   system_done_and_signal(D, tin.prior | need);
+}
+
+template <int DMd>
+__global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
+  drift_phase<DMd>(D, blockIdx.x);
+}
+
+// ------------------------------------------------------ multi-step kernel --
+// A single system whose blocks are all resident at once (a cooperative
+// launch) runs its steps in one kernel: drift phase, grid barrier, force
+// phase, grid barrier, per step. The phases are the kernels' own block
+// functions with the same blocks, so every sum has the same operands in the
+// same order as with one launch per phase: the results are bit for bit those
+// of the per-phase kernels. The kernel returns after the drift of a step that
+// needs a rebuild; the graph around it rebuilds, runs that step's force phase
+// and launches it again for the remaining steps.
+
+// Polls of a grid-barrier wait before it gives up (at least 32 ns each).
+constexpr unsigned kBarrierSpins = 1u << 22;
+
+// Grid-wide barrier. Thread 0 of each block arrives on a counter; the last
+// arrival resets it and advances the generation (release), the others poll
+// the generation (acquire). A wait that runs out of polls records bar_err
+// and returns; the kernel stops at its next check.
+__device__ __forceinline__ void grid_barrier(BatchGlobal* bg, unsigned nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned gen, prev;
+    __threadfence();  // the block's writes (ordered before by the CTA barrier)
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(&bg->bar_gen) : "memory");
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                 : "=r"(prev)
+                 : "l"(&bg->bar_count)
+                 : "memory");
+    if (prev == nblocks - 1) {
+      asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(&bg->bar_count), "r"(0u) : "memory");
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&bg->bar_gen), "r"(gen + 1u)
+                   : "memory");
+    } else {
+      unsigned cur = gen, polls = 0;
+      do {
+        __nanosleep(32);
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                     : "=r"(cur)
+                     : "l"(&bg->bar_gen)
+                     : "memory");
+      } while (cur == gen && ++polls < kBarrierSpins);
+      if (cur == gen) atomicExch(&bg->bar_err, 1);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int ld_volatile(const int32_t* p) { return *(const volatile int32_t*)p; }
+
+// Runs up to bg->steps_left steps of the single system (grid = its blocks).
+// On return bg->steps_left holds the steps not finished (the step whose
+// drift asked for a rebuild counts as not finished); h_rebuild is set when
+// such a step is pending and h_more while steps remain.
+template <int DMd, int FM>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_md_steps(Dev D, cudaGraphConditionalHandle h_more, cudaGraphConditionalHandle h_rebuild) {
+  BatchGlobal* bg = D.bg;
+  const unsigned nb = gridDim.x;
+  const int64_t todo = *(const volatile int64_t*)&bg->steps_left;
+  int64_t done = 0;
+  int rebuild = 0, err = 0;
+  while (done < todo) {
+    drift_phase<DMd>(D, blockIdx.x);
+    grid_barrier(bg, nb);
+    if (ld_volatile(&bg->bar_err)) {
+      err = 1;
+      break;
+    }
+    if (ld_volatile(&bg->any_rebuild)) {
+      rebuild = 1;
+      break;
+    }
+    force_phase<FM, true, false>(D, blockIdx.x);
+    grid_barrier(bg, nb);
+    if (ld_volatile(&bg->bar_err)) {
+      err = 1;
+      break;
+    }
+    ++done;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int64_t left = todo - done;
+    bg->steps_left = left;
+    if (err) D.st->err = 6;  // MDB_ERR_CUDA: a barrier wait gave up
+    cudaGraphSetConditional(h_rebuild, (rebuild && !err) ? 1u : 0u);
+    cudaGraphSetConditional(h_more, (left > 0 && !err) ? 1u : 0u);
+  }
+}
+
+// After the rebuild and the force phase of the pending step.
+__global__ void k_md_steps_count(Dev D, cudaGraphConditionalHandle h_more) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int64_t left = D.bg->steps_left - 1;
+  D.bg->steps_left = left;
+  cudaGraphSetConditional(h_more, left > 0 ? 1u : 0u);
+}
+
+__global__ void k_md_steps_set(Dev D, int64_t n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) D.bg->steps_left = n;
 }
 
 // K = sum 1/2 m |v|^2 (cal_local_K_kernel src/md_cuda_common.cu:554-589) into
