@@ -133,15 +133,17 @@ typedef struct mdb_options {
                              None of these changes any result bit.
                              0 (default): the built-in schedule           */
   int32_t step_kernel;    /* MD steps of a single-system handle:
-                             MDB_STEPS_AUTO (0, default): the multi-step
-                             kernel when every block of the system fits on
-                             the device at once (one cooperative launch runs
-                             the drift and force phases of many steps, with
-                             grid barriers between them) and the system is
-                             small enough that launches dominate a step;
-                             MDB_STEPS_PER_PHASE: one kernel per phase;
-                             MDB_STEPS_MULTI: the multi-step kernel whenever
-                             it fits. Both give the same result bits.       */
+                             MDB_STEPS_AUTO (0, default) or MDB_STEPS_MULTI:
+                             the multi-step kernel when every block of the
+                             system fits on the device at once (two per SM,
+                             so up to ~75k particles on a B200): one
+                             cooperative launch runs the drift and force
+                             phases of many steps with grid barriers between
+                             them and returns only for a cell-list rebuild
+                             (calls of fewer than 4 steps use the per-phase
+                             kernels, whose launch costs less);
+                             MDB_STEPS_PER_PHASE: one kernel per phase.
+                             Both give the same result bits.               */
   int32_t reserved[8];
 } mdb_options_t;
 

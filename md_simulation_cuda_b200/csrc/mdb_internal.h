@@ -34,9 +34,9 @@ constexpr int32_t kListInterior = 1 << 30;
 // Force phase: list rows of the next chunk prefetched into L1 per warp
 // (built-in schedule; Dev::pf_rows holds the one in use).
 constexpr int kListPrefetchRows = 28;
-// MD steps of a single system of at most this many blocks run in the
-// multi-step kernel by default (MDB_STEPS_AUTO).
-constexpr int kMultiStepMaxBlocks = 148;
+// MD calls of at least this many steps use the multi-step kernel where it is
+// enabled (one step: 46 us in it against 36 us per phase at N = 4096).
+constexpr int kMultiStepMinSteps = 4;
 
 // Force-phase variants.
 enum FMode : int32_t {

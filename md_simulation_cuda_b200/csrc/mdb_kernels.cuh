@@ -1381,8 +1381,11 @@ __device__ __forceinline__ int ld_volatile(const int32_t* p) { return *(const vo
 // On return bg->steps_left holds the steps not finished (the step whose
 // drift asked for a rebuild counts as not finished); h_rebuild is set when
 // such a step is pending and h_more while steps remain.
+// (Two blocks per SM: the drift and force phases in one kernel need more
+// than the 64 registers of four, which spilled 270 B; the small systems it
+// serves do not need the occupancy.)
 template <int DMd, int FM>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 2)
     k_md_steps(Dev D, cudaGraphConditionalHandle h_more, cudaGraphConditionalHandle h_rebuild) {
   BatchGlobal* bg = D.bg;
   const unsigned nb = gridDim.x;
