@@ -474,6 +474,11 @@ int mdb_batch_run(mdb_batch_t* b, int64_t iterations);
 int mdb_batch_progress(mdb_batch_t* b, int32_t* n_systems, int32_t* n_done);
 int mdb_batch_system_info(mdb_batch_t* b, int32_t sys_id, int64_t* n, int32_t* done,
                           int64_t* steps);
+/* Cell-list rebuilds of one system so far, and its particles whose neighbour
+ * list overflowed max_neighbors at the last rebuild (they scan the cell
+ * stencil instead). No counterpart in the reference (diagnostics). */
+int mdb_batch_system_stats(mdb_batch_t* b, int32_t sys_id, int64_t* rebuilds,
+                           int32_t* list_overflow);
 int mdb_batch_get_frame(mdb_batch_t* b, int32_t sys_id, mdb_particle_t* out, int64_t n);
 int mdb_batch_get_fire_result(mdb_batch_t* b, int32_t sys_id, mdb_minimize_result_t* result,
                               int32_t* energy_steps, double* energy_trace, int64_t trace_cap);

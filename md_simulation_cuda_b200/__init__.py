@@ -531,10 +531,11 @@ class Batch:
     (add_fire) or MD segments of one kind (add_md)."""
 
     def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True,
-                 fire_precision: Optional[int] = None, autotune: bool = False):
+                 fire_precision: Optional[int] = None, autotune: bool = False,
+                 max_neighbors: Optional[int] = None):
         self._h = C.c_void_p()
-        self._opt = options(device, skin, use_graphs, fire_precision=fire_precision,
-                            autotune=autotune)
+        self._opt = options(device, skin, use_graphs, max_neighbors,
+                            fire_precision=fire_precision, autotune=autotune)
         check(lib().mdb_batch_create(C.byref(self._opt), C.byref(self._h)))
         self._sizes = []
         self._caps = []
@@ -619,6 +620,13 @@ class Batch:
         n, d, st = C.c_int64(), C.c_int32(), C.c_int64()
         check(lib().mdb_batch_system_info(self._h, sys_id, C.byref(n), C.byref(d), C.byref(st)))
         return n.value, bool(d.value), st.value
+
+    def system_stats(self, sys_id: int):
+        """(cell-list rebuilds so far, particles whose list overflowed at the
+        last rebuild) of one system."""
+        r, o = C.c_int64(), C.c_int32()
+        check(lib().mdb_batch_system_stats(self._h, sys_id, C.byref(r), C.byref(o)))
+        return r.value, o.value
 
     def device_bytes(self) -> int:
         b = C.c_int64()

@@ -316,6 +316,7 @@ SIGNATURES = {
     "mdb_batch_run": ([_vp, C.c_int64], C.c_int),
     "mdb_batch_progress": ([_vp, _ip, _ip], C.c_int),
     "mdb_batch_system_info": ([_vp, C.c_int32, C.POINTER(C.c_int64), _ip, C.POINTER(C.c_int64)], C.c_int),
+    "mdb_batch_system_stats": ([_vp, C.c_int32, C.POINTER(C.c_int64), _ip], C.c_int),
     "mdb_batch_get_frame": ([_vp, C.c_int32, _vp, C.c_int64], C.c_int),
     "mdb_batch_get_fire_result": ([_vp, C.c_int32, C.POINTER(MDBMinimizeResult), _ip, _dp, C.c_int64], C.c_int),
     "mdb_batch_energies": ([_vp, C.c_int32, _dp, _dp, _dp], C.c_int),

@@ -1033,6 +1033,18 @@ int mdb_batch_system_info(mdb_batch_t* b, int32_t sys_id, int64_t* n, int32_t* d
   return MDB_OK;
 }
 
+int mdb_batch_system_stats(mdb_batch_t* b, int32_t sys_id, int64_t* rebuilds,
+                           int32_t* list_overflow) {
+  if (!b) return mdb::set_error(MDB_ERR_ARG, "null argument");
+  MDB_TRY(batch_build(b));
+  if (sys_id < 0 || sys_id >= b->eng->nsys()) return mdb::set_error(MDB_ERR_ARG, "bad system id");
+  SysState S;
+  MDB_TRY(b->eng->get_state(sys_id, &S));
+  if (rebuilds) *rebuilds = S.rebuilds;
+  if (list_overflow) *list_overflow = S.nl_overflow;
+  return MDB_OK;
+}
+
 int mdb_batch_get_frame(mdb_batch_t* b, int32_t sys_id, mdb_particle_t* out, int64_t n) {
   if (!b || !out) return mdb::set_error(MDB_ERR_ARG, "null argument");
   MDB_TRY(batch_build(b));

@@ -257,6 +257,7 @@ int Engine::build() {
     S.f_dt = sp.fire.dt_init;
     S.f_alpha = sp.fire.alpha0;
     S.f_fp64 = (sp.kind == K_FIRE && fire_prec_ == MDB_FIRE_FP64) ? 1 : 0;
+    S.rb_last = kNoRebuildYet;
     p0 += n;
     b0 += P.nb;
     c0 += (int64_t)P.ccap_x * P.ccap_y;

@@ -104,7 +104,18 @@ struct SysState {
   int32_t f_drift;  // the force phase of this iteration ran and did not converge
   int32_t f_fp64;   // FP64 pair terms for this system (FIRE and its observations)
   int32_t f_pad;
+  // step (MD) or iteration (FIRE) counter at the last rebuild that the drift
+  // asked for; a forced rebuild resets it to kNoRebuildYet
+  int64_t rb_last;
 };
+
+// SysState::rb_last before any drift-requested rebuild.
+constexpr int64_t kNoRebuildYet = -(int64_t(1) << 40);
+// A rebuild builds the system's neighbour list only when its previous
+// drift-requested rebuild is at least this many steps (iterations) back;
+// otherwise its force phase scans the cell stencil until the next rebuild
+// (a list rebuilt every step or two costs more than it saves).
+constexpr int64_t kListMinReuse = 3;
 
 struct BatchGlobal {
   int32_t any_rebuild;
@@ -115,7 +126,7 @@ struct BatchGlobal {
   uint32_t bar_count;  // multi-step kernel: grid barrier arrivals
   uint32_t bar_gen;    //   and generation
   int32_t bar_err;     //   a barrier wait ran out of polls
-  int32_t pad;
+  int32_t forced;      // the pending rebuild was forced (not asked for by a drift)
 };
 
 // The NPH driver protocol (run_test_NPH.cpp:137-290) run on the device: its

@@ -1770,15 +1770,25 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
   return cnt;
 }
 
+// Steps (MD) or iterations (FIRE) the system has run: the clock of its
+// rebuild history.
+__device__ __forceinline__ int64_t rebuild_clock(const SysParams& P, const SysState& S) {
+  return P.kind == K_FIRE ? (int64_t)S.f_step : S.steps;
+}
+
 __global__ void k_rb_nlist(Dev D) {
   if (!rebuild_requested(D)) return;
+  const bool forced = *((volatile int*)&D.bg->forced) != 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < D.ntot; k += stride) {
     const int s = D.sysid[k];
     if (!sys_rebuilds(D, s)) continue;
     const SysParams& P = D.sp[s];
     SysState* S = D.st + s;
-    if (S->allpairs || D.max_nbr <= 0) {
+    // a system that rebuilds again within kListMinReuse steps scans its cell
+    // stencil instead of a list it would hardly reuse
+    const bool recent = !forced && rebuild_clock(P, *S) - S->rb_last < kListMinReuse;
+    if (S->allpairs || D.max_nbr <= 0 || recent) {
       D.ncount[k] = -1;
       continue;
     }
@@ -1809,6 +1819,7 @@ __global__ void k_rb_nlist(Dev D) {
 
 __global__ void k_rb_finish(Dev D) {
   if (!rebuild_requested(D)) return;
+  const bool forced = *((volatile int*)&D.bg->forced) != 0;
   for (int s = threadIdx.x; s < D.nsys; s += blockDim.x) {
     SysState* S = D.st + s;
     if (!S->need_rebuild) continue;
@@ -1817,9 +1828,13 @@ __global__ void k_rb_finish(Dev D) {
     S->dmax_y = 0u;
     S->jump = 0u;
     S->rebuilds += 1;
+    S->rb_last = forced ? kNoRebuildYet : rebuild_clock(D.sp[s], *S);
   }
   __syncthreads();
-  if (threadIdx.x == 0) D.bg->any_rebuild = 0;
+  if (threadIdx.x == 0) {
+    D.bg->any_rebuild = 0;
+    D.bg->forced = 0;
+  }
 }
 
 // ------------------------------------------------------------ profiles --
@@ -2020,7 +2035,10 @@ __global__ void k_force_rebuild(Dev D, int periodic_y) {
     D.st[s].need_rebuild = 1;
     if (periodic_y >= 0) D.st[s].periodic_y = periodic_y;
   }
-  if (threadIdx.x == 0) D.bg->any_rebuild = 1;
+  if (threadIdx.x == 0) {
+    D.bg->any_rebuild = 1;
+    D.bg->forced = 1;
+  }
 }
 
 __global__ void k_set_pext(Dev D, double p) {

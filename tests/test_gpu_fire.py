@@ -132,6 +132,9 @@ def test_batch_equals_solo(built):
         assert np.array_equal(rb.frame["pos"], solo.frame["pos"], equal_nan=True)
         assert np.array_equal(rb.energy_trace, solo.energy_trace, equal_nan=True)
         assert rb.nonfinite == solo.nonfinite
+        # every system was binned at build and rebuilt on its own schedule after
+        rebuilds, overflow = b.system_stats(k)
+        assert 1 <= rebuilds <= rb.steps + 1 and overflow >= 0
 
 
 def test_fire_reaches_1e6_from_random_starts(built):
