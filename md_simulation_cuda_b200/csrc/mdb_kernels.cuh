@@ -19,12 +19,35 @@ namespace mdb {
 // pbc_wrap_hd (include/md_cuda_common.hpp:20-29): fmod(x, L), then + L when
 // negative. For -L <= x < 2L the branches below give the same bits as fmod
 // (x - L is exact there), which covers every step but pathological jumps.
+// Exact remainder of x by L with the sign of x (the value fmod returns), for
+// finite x, L. Each pass removes up to 40 bits of the quotient: with
+// y = |L| 2^k and r / y < 2^41, q = floor(fl(r / y)) is the true quotient or
+// one more (rounding to nearest never falls below an integer the true value
+// reaches), so r - q y lies in [-y, y), is a multiple of ulp(y) and is
+// computed exactly by one fma; adding y back to a negative remainder is exact
+// as well. A particle that jumps 2^90 box lengths in one step (a FIRE start
+// with overlapping pairs) takes 3 passes.
+__device__ __noinline__ double fmod_exact(double x, double L) {
+  if (!isfinite(x) || !isfinite(L) || L == 0.0) return fmod(x, L);
+  const double a = fabs(L);
+  double r = fabs(x);
+  for (int pass = 0; r >= a && pass < 64; ++pass) {
+    const int e = ilogb(r) - ilogb(a);
+    const double y = ldexp(a, e > 40 ? e - 40 : 0);
+    const double q = floor(r / y);
+    double rem = fma(-q, y, r);
+    if (rem < 0.0) rem += y;
+    r = rem;
+  }
+  return copysign(r, x);
+}
+
 __device__ __forceinline__ double pbc_wrap(double x, double L) {
   if (L <= 0.0) return x;
   if (x >= 0.0 && x < L) return x;
   if (x >= L && x < 2.0 * L) return x - L;
   if (x < 0.0 && x >= -L) return x + L;
-  x = fmod(x, L);
+  x = fmod_exact(x, L);
   if (x < 0.0) x += L;
   return x;
 }

@@ -226,3 +226,46 @@ def test_fire_close_pair_stays_finite(built):
     sr2 = 1.0 / r2
     tmp = 24.0 * (2.0 * sr2 ** 6 - sr2 ** 3) / r2
     assert abs(res.frame["acc"][0, 0] / (tmp * 0.001) + 1.0) < 1e-4
+
+
+def _wrap_ref(x, L):
+    """pbc_wrap_hd (include/md_cuda_common.hpp:20-29) in host arithmetic:
+    C fmod is exact, then + L for a negative remainder."""
+    import math
+
+    if 0.0 <= x < L:
+        return x
+    if L <= x < 2.0 * L:
+        return x - L
+    if -L <= x < 0.0:
+        return x + L
+    r = math.fmod(x, L)
+    return r + L if r < 0.0 else r
+
+
+def test_fire_entry_wraps_far_positions_exactly(built):
+    """The FIRE entry wraps every position into the box; positions many box
+    lengths out (a random start's overlapping pair can throw a particle
+    2^90 box lengths in one step) wrap bit for bit as the host's exact fmod
+    does."""
+    rng = np.random.default_rng(11)
+    n = 64
+    L = 9.87654321
+    f = mdb.make_frame(n)
+    far = [1e25, -3.7e18, 5.5 * L + 1e-9, -1e300, 2.0 ** 90 + 0.5, -(2.0 ** 60) * L,
+           7.0 * L, -7.0 * L, 1e-300, 3e8 * L + 0.25, -1.5 * L, 1.999 * L]
+    xs = np.concatenate([far, rng.uniform(-1e40, 1e40, n - len(far))])
+    ys = rng.uniform(-1e12, 1e12, n)
+    f["pos"][:, 0] = xs
+    f["pos"][:, 1] = ys
+    f["type"] = rng.integers(0, 2, n)
+    cfgd = wl.config_dict(n, L, L, dt=0.001)
+    mgr = mdb.MDConfigManager(mdb._lib.MDBConfigC())
+    for k, v in cfgd.items():
+        setattr(mgr.config, k, v)
+    mgr.config.n_cap = n
+    res = mdb.EnergyMinimizer(mgr).minimize_frame(f, 1e300, 1,
+                                               mdb.FireParams(dt_init=0.001, dt_max=0.01))
+    got = res.frame["pos"]
+    want = np.array([[_wrap_ref(float(x), L), _wrap_ref(float(y), L)] for x, y in zip(xs, ys)])
+    assert np.array_equal(got, want)
