@@ -993,7 +993,10 @@ bool cache_lookup(const std::string& key, int* pf, int* nlg, int* rbg) {
     if (tab == std::string::npos || line.compare(0, tab, key) != 0 || tab != key.size()) continue;
     std::istringstream vs(line.substr(tab + 1));
     int a, b, c;
-    if (vs >> a >> b >> c) {
+    // (several processes may append to the file at once: a line that does not
+    // hold a plausible schedule is skipped)
+    if ((vs >> a >> b >> c) && a >= 0 && a <= 32 && b >= 1 && b <= (1 << 20) && c >= 1 &&
+        c <= (1 << 20)) {
       *pf = a;
       *nlg = b;
       *rbg = c;
@@ -1005,8 +1008,15 @@ bool cache_lookup(const std::string& key, int* pf, int* nlg, int* rbg) {
 
 void cache_store(const std::string& key, int pf, int nlg, int rbg) {
   std::lock_guard<std::mutex> lk(g_cache_mu);
+  // one write of the whole line (appends of a short line are atomic between
+  // processes)
+  std::ostringstream line;
+  line << key << '\t' << pf << ' ' << nlg << ' ' << rbg << '\n';
   std::ofstream out(cache_path(), std::ios::app);
-  if (out) out << key << '\t' << pf << ' ' << nlg << ' ' << rbg << '\n';
+  if (out) {
+    const std::string t = line.str();
+    out.write(t.data(), (std::streamsize)t.size());
+  }
 }
 
 int bucket(int64_t x) {  // log2 bucket of a size
