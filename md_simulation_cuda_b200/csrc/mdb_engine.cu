@@ -19,35 +19,41 @@
 
 namespace mdb {
 
-void* force_fn(int fm, bool py) {
-#define MDB_F(M) return py ? (void*)k_force<M, true> : (void*)k_force<M, false>
+void* force_fn(int fm, bool py, bool ln) {
+#define MDB_F(M)                                                                 \
+  return ln ? (py ? (void*)k_force<M, true, true> : (void*)k_force<M, false, true>) \
+            : (py ? (void*)k_force<M, true, false> : (void*)k_force<M, false, false>)
   switch (fm) {
     case FM_INIT: MDB_F(FM_INIT);
     case FM_NVE: MDB_F(FM_NVE);
     case FM_NH: MDB_F(FM_NH);
     case FM_NPH: MDB_F(FM_NPH);
     case FM_PISTON: MDB_F(FM_PISTON);
-    case FM_FIRE: MDB_F(FM_FIRE);
+    // FIRE systems keep one lane per slot
+    case FM_FIRE: return py ? (void*)k_force<FM_FIRE, true, false> : (void*)k_force<FM_FIRE, false, false>;
     default: MDB_F(FM_OBS);
   }
 #undef MDB_F
 }
 
-void* drift_fn(int dm) {
+void* drift_fn(int dm, bool ln) {
   switch (dm) {
-    case DM_NVE: return (void*)k_drift<DM_NVE>;
-    case DM_NH: return (void*)k_drift<DM_NH>;
-    case DM_NPH: return (void*)k_drift<DM_NPH>;
-    case DM_PISTON: return (void*)k_drift<DM_PISTON>;
-    default: return (void*)k_drift<DM_FIRE>;
+    case DM_NVE: return ln ? (void*)k_drift<DM_NVE, true> : (void*)k_drift<DM_NVE, false>;
+    case DM_NH: return ln ? (void*)k_drift<DM_NH, true> : (void*)k_drift<DM_NH, false>;
+    case DM_NPH: return ln ? (void*)k_drift<DM_NPH, true> : (void*)k_drift<DM_NPH, false>;
+    case DM_PISTON: return ln ? (void*)k_drift<DM_PISTON, true> : (void*)k_drift<DM_PISTON, false>;
+    default: return (void*)k_drift<DM_FIRE, false>;
   }
 }
 
-void* steps_fn(int dm) {
+void* steps_fn(int dm, bool ln) {
   switch (dm) {
-    case DM_NVE: return (void*)k_md_steps<DM_NVE, FM_NVE>;
-    case DM_NH: return (void*)k_md_steps<DM_NH, FM_NH>;
-    default: return (void*)k_md_steps<DM_NPH, FM_NPH>;
+    case DM_NVE: return ln ? (void*)k_md_steps<DM_NVE, FM_NVE, true>
+                           : (void*)k_md_steps<DM_NVE, FM_NVE, false>;
+    case DM_NH: return ln ? (void*)k_md_steps<DM_NH, FM_NH, true>
+                          : (void*)k_md_steps<DM_NH, FM_NH, false>;
+    default: return ln ? (void*)k_md_steps<DM_NPH, FM_NPH, true>
+                       : (void*)k_md_steps<DM_NPH, FM_NPH, false>;
   }
 }
 
@@ -175,10 +181,19 @@ int Engine::build() {
     maxn = std::max<int64_t>(maxn, n);
     P.p0 = p0;
     P.n = n;
+    // MDB_LANES=<1|4> fixes the lanes per slot (tuning aid; 0 = automatic).
+    const char* lanes_env = getenv("MDB_LANES");
+    const int lanes_fixed = lanes_env ? atoi(lanes_env) : 0;
+    P.lanes = (lanes_fixed == 1 || lanes_fixed == kLanes)
+                  ? lanes_fixed
+                  : ((sp.kind != K_FIRE && n <= kLanesMaxN) ? kLanes : 1);
+    const int spb = kThreads / P.lanes;  // slots per block and pass
     P.items = items_fixed > 0
                   ? std::min(items_fixed, kMaxItems)
                   : (int)std::min<int64_t>(kMaxItems, std::max<int64_t>(1, (n + wave - 1) / wave));
-    P.nb = (n + kThreads * P.items - 1) / (kThreads * P.items);
+    if (P.lanes > 1) P.items = 1;
+    if (P.lanes > 1) lanes_ = true;
+    P.nb = (n + spb * P.items - 1) / (spb * P.items);
     P.b0 = b0;
     P.kind = sp.kind;
     P.sig[0] = c.SIGMA_AA;
@@ -433,7 +448,7 @@ int Engine::choose_multi_step() {
   int per_sm = 1 << 30;
   for (int dm : {DM_NVE, DM_NH, DM_NPH}) {
     int b = 0;
-    MDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, steps_fn(dm), kThreads, 0));
+    MDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, steps_fn(dm, lanes_), kThreads, 0));
     per_sm = std::min(per_sm, b);
   }
   multi_cap_ = per_sm * nsm;
@@ -477,7 +492,7 @@ int Engine::get_steps_graph(int dm, int fm, cudaGraphExec_t* exec) {
   if (rc == MDB_OK) {
     void* args[] = {&d, &h_more, &h_rb};
     cudaKernelNodeParams kp = {};
-    kp.func = steps_fn(dm);
+    kp.func = steps_fn(dm, lanes_);
     kp.gridDim = dim3(nblocks_);
     kp.blockDim = dim3(kThreads);
     kp.kernelParams = args;
@@ -514,7 +529,7 @@ int Engine::get_steps_graph(int dm, int fm, cudaGraphExec_t* exec) {
     if (rc == MDB_OK && !last) rc = set_error(MDB_ERR_STATE, "rebuild body has no last node");
     cudaGraphNode_t nf, nc;
     if (rc == MDB_OK)
-      rc = add_kernel_node(rb_body, &last, 1, force_fn(fm, true), nblocks_, kThreads, dev_, &nf);
+      rc = add_kernel_node(rb_body, &last, 1, force_fn(fm, true, lanes_), nblocks_, kThreads, dev_, &nf);
     if (rc == MDB_OK) {
       void* args[] = {&d, &h_more};
       cudaKernelNodeParams kp = {};
@@ -583,7 +598,7 @@ int Engine::set_pext(double p) {
 
 int Engine::force(int fm, bool py) {
   MDB_CUDA(cudaSetDevice(device_));
-  return launch(force_fn(fm, py), nblocks_, kThreads, dev_);
+  return launch(force_fn(fm, py, lanes_), nblocks_, kThreads, dev_);
 }
 
 int Engine::reduce_K() {
@@ -678,15 +693,15 @@ int Engine::get_graph(int kind, int dm, int fm, bool py, int chunk, cudaGraphExe
     dd.use_cond = 1;
     cudaGraphNode_t nd, nc, nf;
     if (kind == 0) {
-      rc = add_kernel_node(g, prev ? &prev : nullptr, prev ? 1 : 0, drift_fn(dm), nblocks_,
+      rc = add_kernel_node(g, prev ? &prev : nullptr, prev ? 1 : 0, drift_fn(dm, lanes_), nblocks_,
                            kThreads, dd, &nd);
       if (!rc) rc = add_cond_rebuild(g, nd, h, &nc);
-      if (!rc) rc = add_kernel_node(g, &nc, 1, force_fn(fm, py), nblocks_, kThreads, dev_, &nf);
+      if (!rc) rc = add_kernel_node(g, &nc, 1, force_fn(fm, py, lanes_), nblocks_, kThreads, dev_, &nf);
       prev = nf;
     } else {
-      rc = add_kernel_node(g, prev ? &prev : nullptr, prev ? 1 : 0, force_fn(FM_FIRE, true),
+      rc = add_kernel_node(g, prev ? &prev : nullptr, prev ? 1 : 0, force_fn(FM_FIRE, true, lanes_),
                            nblocks_, kThreads, dev_, &nf);
-      if (!rc) rc = add_kernel_node(g, &nf, 1, drift_fn(DM_FIRE), nblocks_, kThreads, dd, &nd);
+      if (!rc) rc = add_kernel_node(g, &nf, 1, drift_fn(DM_FIRE, lanes_), nblocks_, kThreads, dd, &nd);
       if (!rc) rc = add_cond_rebuild(g, nd, h, &nc);
       prev = nc;
     }
@@ -745,9 +760,9 @@ int Engine::run_md(int dm, int fm, bool py, int64_t nsteps) {
   }
   for (; left > 0; --left) {
     int rc;
-    if ((rc = launch(drift_fn(dm), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch(drift_fn(dm, lanes_), nblocks_, kThreads, dev_))) return rc;
     if ((rc = launch_rebuild_eager())) return rc;
-    if ((rc = launch(force_fn(fm, py), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch(force_fn(fm, py, lanes_), nblocks_, kThreads, dev_))) return rc;
   }
   return MDB_OK;
 }
@@ -761,11 +776,11 @@ int Engine::run_md_timed(int dm, int fm, bool py, int64_t nsteps, double* ms) {
   int rc = MDB_OK;
   for (int64_t s = 0; s < nsteps && rc == MDB_OK; ++s) {
     cudaEventRecord(ev[0], stream_);
-    rc = launch(drift_fn(dm), nblocks_, kThreads, dev_);
+    rc = launch(drift_fn(dm, lanes_), nblocks_, kThreads, dev_);
     cudaEventRecord(ev[1], stream_);
     if (!rc) rc = launch_rebuild_eager();
     cudaEventRecord(ev[2], stream_);
-    if (!rc) rc = launch(force_fn(fm, py), nblocks_, kThreads, dev_);
+    if (!rc) rc = launch(force_fn(fm, py, lanes_), nblocks_, kThreads, dev_);
     cudaEventRecord(ev[3], stream_);
     cudaError_t e = cudaEventSynchronize(ev[3]);
     if (e != cudaSuccess) {
@@ -807,8 +822,8 @@ int Engine::run_fire(int64_t iters) {
   }
   for (; left > 0; --left) {
     int rc;
-    if ((rc = launch(force_fn(FM_FIRE, true), nblocks_, kThreads, dev_))) return rc;
-    if ((rc = launch(drift_fn(DM_FIRE), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch(force_fn(FM_FIRE, true, lanes_), nblocks_, kThreads, dev_))) return rc;
+    if ((rc = launch(drift_fn(DM_FIRE, lanes_), nblocks_, kThreads, dev_))) return rc;
     if ((rc = launch_rebuild_eager())) return rc;
   }
   return MDB_OK;
@@ -1034,11 +1049,11 @@ int Engine::time_force(int fm, int reps, double* ms) {
   cudaEvent_t a, b;
   MDB_CUDA(cudaEventCreate(&a));
   MDB_CUDA(cudaEventCreate(&b));
-  int rc = launch(force_fn(fm, true), nblocks_, kThreads, dev_);  // warm
+  int rc = launch(force_fn(fm, true, lanes_), nblocks_, kThreads, dev_);  // warm
   double best = 1e30;
   for (int r = 0; !rc && r < reps; ++r) {
     cudaEventRecord(a, stream_);
-    rc = launch(force_fn(fm, true), nblocks_, kThreads, dev_);
+    rc = launch(force_fn(fm, true, lanes_), nblocks_, kThreads, dev_);
     cudaEventRecord(b, stream_);
     cudaEventSynchronize(b);
     float t = 0.f;

@@ -150,6 +150,7 @@ class Engine {
   int autotune_ = 0;
   int step_kernel_ = MDB_STEPS_AUTO;
   bool multi_step_ = false;
+  bool lanes_ = false;  // some system has several lanes per slot (SysParams::lanes)
   int multi_cap_ = 0;  // blocks of the multi-step kernel the device holds at once
   mdb_schedule_t schedule_{};
   int stream_priority_ = 0;  // levels above normal for stream_
@@ -168,9 +169,10 @@ class Engine {
   long long last_rebuilds_ = 0;
 };
 
-// Kernel of a force phase (FM_*; py: periodic y) and of a drift phase (DM_*).
-void* force_fn(int fm, bool py);
-void* drift_fn(int dm);
+// Kernel of a force phase (FM_*; py: periodic y) and of a drift phase (DM_*);
+// ln: the launch holds systems with several lanes per slot.
+void* force_fn(int fm, bool py, bool ln);
+void* drift_fn(int dm, bool ln);
 
 int reference_initial_frame(const mdb_config_t& cfg, std::vector<mdb_particle_t>& out);
 

@@ -34,6 +34,12 @@ constexpr int32_t kListInterior = 1 << 30;
 // Force phase: list rows of the next chunk prefetched into L1 per warp
 // (built-in schedule; Dev::pf_rows holds the one in use).
 constexpr int kListPrefetchRows = 28;
+// Small MD systems (n <= kLanesMaxN) give each slot kLanes lanes of the force
+// phase, which split its pair candidates; a block then covers kThreads /
+// kLanes slots in every phase. A rule on the system alone, so a system gets
+// the same bits alone and in a batch. FIRE systems keep one lane per slot.
+constexpr int kLanes = 4;
+constexpr int kLanesMaxN = 16384;
 // MD calls of at least this many steps use the multi-step kernel where it is
 // enabled (one step: 46 us in it against 36 us per phase at N = 4096).
 constexpr int kMultiStepMinSteps = 4;
@@ -64,6 +70,7 @@ struct SysParams {
   int32_t items;  // particles per thread (a block covers kThreads*items slots)
   int32_t ccap_x, ccap_y;
   int32_t kind;
+  int32_t lanes;  // lanes per slot in the force phase (1, or kLanes for small MD systems)
   float frl2[3];  // neighbour-list radius^2 per pair class: (rc_ij + skin)^2
   double sig[3], eps[3], Vc[3];  // AA, BB, AB
   double massA, massB, cutoff, rc_max, r_cell, skin;

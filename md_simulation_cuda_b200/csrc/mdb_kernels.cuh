@@ -434,22 +434,27 @@ __device__ __forceinline__ float4 ld_pos(const float4* p) {
   return v;
 }
 
-template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, bool FLOOR, bool NC, typename IDX>
+// LANES > 1: the slot's list is shared by LANES lanes; lane `lane` takes the
+// entries lane, lane + LANES, ... (the caller adds the lanes' sums).
+template <bool PY, bool ENERGY, bool VIRIAL, bool MIC, bool FLOOR, bool NC, int LANES = 1,
+          typename IDX>
 __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
                                           const IDX* __restrict__ nlist, int64_t ntot, int64_t i,
                                           int li, int n, int nn, const PairCtx& c, float2& fs,
                                           float2& fc, float& ws, float& wc, double& u,
-                                          double& an) {
-  const IDX* __restrict__ p = nlist + i;
+                                          double& an, int lane = 0) {
+  const IDX* __restrict__ p = nlist + i + (int64_t)lane * ntot;
   // MIC: slot 0 of the system and a wrapped index; interior: slot i itself
   const float4* __restrict__ base = MIC ? pff + (i - li) : pff + i;
-  constexpr int PF = (ENERGY || VIRIAL) ? 4 : 8;  // prefetch width (register budget)
+  constexpr int PF = (LANES > 1) ? 4 : ((ENERGY || VIRIAL) ? 4 : 8);  // prefetch width
+  const int64_t step = (int64_t)LANES * ntot;
+  nn = (LANES > 1) ? (nn > lane ? (nn - lane + LANES - 1) / LANES : 0) : nn;
   int k = 0;
   for (; k + PF <= nn; k += PF) {
     int j[PF];
 #pragma unroll
     for (int q = 0; q < PF; ++q) {
-      int t = (int)__ldg(p + (int64_t)(k + q) * ntot);
+      int t = (int)__ldg(p + (int64_t)(k + q) * step);
       if (MIC) {
         t += li;
         t += (t < 0) ? n : 0;
@@ -462,7 +467,7 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
       pair_one<PY, ENERGY, VIRIAL, MIC, FLOOR>(ld_pos<NC>(base + j[q]), c, fs, fc, ws, wc, u, an);
   }
   for (; k < nn; ++k) {
-    int t = (int)__ldg(p + (int64_t)k * ntot);
+    int t = (int)__ldg(p + (int64_t)k * step);
     if (MIC) {
       t += li;
       t += (t < 0) ? n : 0;
@@ -473,12 +478,12 @@ __device__ __forceinline__ void pair_list(const float4* __restrict__ pff,
 }
 
 // Candidates j in [j0, j1) (cell stencil rows or the whole system).
-template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR, bool NC>
+template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR, bool NC, int LANES = 1>
 __device__ __forceinline__ void pair_range(const float4* __restrict__ pff, int j0, int j1,
                                            const PairCtx& c, float2& fs, float2& fc, float& ws,
-                                           float& wc, double& u, double& an) {
+                                           float& wc, double& u, double& an, int lane = 0) {
 #pragma unroll 4
-  for (int j = j0; j < j1; ++j)
+  for (int j = j0 + lane; j < j1; j += LANES)
     pair_one<PY, ENERGY, VIRIAL, true, FLOOR>(ld_pos<NC>(pff + j), c, fs, fc, ws, wc, u, an);
 }
 
@@ -522,11 +527,14 @@ __device__ __forceinline__ void set_profile_class(PairCtx& c, const SysParams& P
 // system for grids narrower than 3 cells). Returns F in FP64. tci receives the
 // type class of slot i, decoded from its float-float position (encode_ff), so
 // the type array is not read.
-template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR = false, bool NC = true>
+//
+// LANES > 1: lane `lane` of the LANES lanes that share slot i sums its share
+// of the candidates (the caller adds the lanes' results in a fixed order).
+template <bool PY, bool ENERGY, bool VIRIAL, bool FLOOR = false, bool NC = true, int LANES = 1>
 __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P, const SysState& S,
                                                int64_t i, double Lx, double Ly, double& fx,
                                                double& fy, double& w, double& u, double& an,
-                                               int& tci) {
+                                               int& tci, int lane = 0) {
   PairCtx c;
   const float4 qi = ld_pos<NC>(D.pff + i);
   set_pair_box<PY>(c, qi, Lx, Ly);
@@ -561,22 +569,22 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
     const int nn = nc & (kListInterior - 1);
     if (D.nl16) {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false, FLOOR, NC>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
-                                                  wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR, NC, LANES>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs,
+                                                  fc, ws, wc, u, an, lane);
       else
-        pair_list<PY, ENERGY, VIRIAL, true, FLOOR, NC>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
-                                                 wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR, NC, LANES>(pff, D.nlist16, D.ntot, i, li, P.n, nn, c, fs,
+                                                 fc, ws, wc, u, an, lane);
     } else {
       if (nc & kListInterior)
-        pair_list<PY, ENERGY, VIRIAL, false, FLOOR, NC>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
-                                                  wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, false, FLOOR, NC, LANES>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs,
+                                                  fc, ws, wc, u, an, lane);
       else
-        pair_list<PY, ENERGY, VIRIAL, true, FLOOR, NC>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs, fc, ws,
-                                                 wc, u, an);
+        pair_list<PY, ENERGY, VIRIAL, true, FLOOR, NC, LANES>(pff, D.nlist, D.ntot, i, li, P.n, nn, c, fs,
+                                                 fc, ws, wc, u, an, lane);
     }
   } else if (S.allpairs) {
-    pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fs, fc, ws, wc,
-                                          u, an);
+    pair_range<PY, ENERGY, VIRIAL, FLOOR, NC, LANES>(pff, (int)P.p0, (int)(P.p0 + P.n), c, fs, fc, ws, wc,
+                                          u, an, lane);
   } else {
     const int ncx = S.ncx, ncy = S.ncy;
     const int cell = D.cell_of[i];
@@ -593,18 +601,18 @@ __device__ __forceinline__ void particle_force(const Dev& D, const SysParams& P,
       }
       const int64_t row = P.c0 + (int64_t)yy * ncx;
       if (cx > 0 && cx < ncx - 1) {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row + cx - 1),
-                                              __ldg(cs + row + cx + 2), c, fs, fc, ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC, LANES>(pff, __ldg(cs + row + cx - 1),
+                                              __ldg(cs + row + cx + 2), c, fs, fc, ws, wc, u, an, lane);
       } else if (cx == 0) {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fs, fc,
-                                              ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row + ncx - 1),
-                                              __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC, LANES>(pff, __ldg(cs + row), __ldg(cs + row + 2), c, fs, fc,
+                                              ws, wc, u, an, lane);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC, LANES>(pff, __ldg(cs + row + ncx - 1),
+                                              __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an, lane);
       } else {
-        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row + ncx - 2),
-                                              __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an);
-        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fs, fc,
-                                              ws, wc, u, an);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC, LANES>(pff, __ldg(cs + row + ncx - 2),
+                                              __ldg(cs + row + ncx), c, fs, fc, ws, wc, u, an, lane);
+        pair_range<PY, ENERGY, VIRIAL, FLOOR, NC, LANES>(pff, __ldg(cs + row), __ldg(cs + row + 1), c, fs, fc,
+                                              ws, wc, u, an, lane);
       }
     }
   }
@@ -906,12 +914,12 @@ __device__ __noinline__ ForceFinish<FM, PY> force_items_hp(Dev D, const SysParam
 // force_phase is the work of block b of the launch; k_force runs it as one
 // kernel, k_md_steps as a phase of its multi-step loop (NC = false: plain
 // position loads, see ld_pos).
-template <int FM, bool PY, bool NC>
+template <int FM, bool PY, bool NC, bool LN>
 __device__ __forceinline__ void force_phase(const Dev& D, const int b) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
-  {
+  if (!LN || P.lanes == 1) {
     // L1 prefetch of this thread's first slot and its first list rows
     const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * kThreads + threadIdx.x;
     if (i0 < P.p0 + P.n) {
@@ -947,6 +955,31 @@ __device__ __forceinline__ void force_phase(const Dev& D, const int b) {
   ForceFinish<FM, PY> fin;
   if (kHpCapable && !skip && S->f_fp64 != 0) {
     fin = force_items_hp<FM, PY>(D, &P, S, base, stride, end, items, Lx, Ly, h, xi2, fdt);
+  } else if (LN && P.lanes == kLanes) {
+    // kLanes lanes per slot: a block covers kThreads / kLanes slots; the
+    // lanes of a slot split its candidates, their sums are added in a fixed
+    // butterfly (every lane ends with the same bits) and the first lane
+    // finishes the slot. items is 1 for these systems.
+    fin.init();
+    constexpr int spb = kThreads / kLanes;
+    const int lane = threadIdx.x % kLanes;
+    const int64_t i = P.p0 + (int64_t)(b - P.b0) * spb + threadIdx.x / kLanes;
+    double fx = 0.0, fy = 0.0, w = 0.0, u = 0.0, an = 0.0;
+    int tci = 0;
+    if (!skip && i < end)
+      particle_force<PY, kEnergy, kVirial, kHpCapable, NC, kLanes>(D, P, *S, i, Lx, Ly, fx, fy, w,
+                                                                 u, an, tci, lane);
+#pragma unroll
+    for (int o = 1; o < kLanes; o <<= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);
+      if (kVirial) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if (kEnergy) {
+        u += __shfl_xor_sync(0xffffffffu, u, o);
+        an += __shfl_xor_sync(0xffffffffu, an, o);
+      }
+    }
+    if (!skip && i < end && lane == 0) fin(D, P, Ly, h, xi2, fdt, i, fx, fy, w, u, an, tci);
   } else {
     fin.init();
     const int q_first = b - P.b0;
@@ -1081,9 +1114,11 @@ __device__ __forceinline__ void force_phase(const Dev& D, const int b) {
   S->counter = 0u;
 }
 
-template <int FM, bool PY>
+// LN: the launch holds systems with several lanes per slot (the kernel
+// without them keeps the one-lane code only).
+template <int FM, bool PY, bool LN>
 __global__ void __launch_bounds__(kThreads, 4) k_force(Dev D) {
-  force_phase<FM, PY, true>(D, blockIdx.x);
+  force_phase<FM, PY, true, LN>(D, blockIdx.x);
 }
 
 // ------------------------------------------------------------ drift phase --
@@ -1174,7 +1209,7 @@ __device__ __forceinline__ void drift_particle(const Dev& D, const DriftCtx& c, 
 
 // drift_phase is the work of block b of the launch (k_drift: one kernel;
 // k_md_steps: a phase of its multi-step loop).
-template <int DMd>
+template <int DMd, bool LN>
 __device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
   const int s = D.sys_of_block[b];
   const SysParams& P = D.sp[s];
@@ -1182,8 +1217,9 @@ __device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
   {
     // L1 prefetch of this thread's first particle: its DRAM latency overlaps
     // the scalar prologue below
-    const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * kThreads * P.items + threadIdx.x;
-    if (i0 < P.p0 + P.n) {
+    const int spb0 = LN ? kThreads / P.lanes : kThreads;
+    const int64_t i0 = P.p0 + (int64_t)(b - P.b0) * spb0 * P.items + threadIdx.x;
+    if ((int)threadIdx.x < spb0 && i0 < P.p0 + P.n) {
       asm volatile("prefetch.global.L1 [%0];" ::"l"(D.pos + i0));
       asm volatile("prefetch.global.L1 [%0];" ::"l"(D.vel + i0));
       asm volatile("prefetch.global.L1 [%0];" ::"l"(D.acc + i0));
@@ -1259,8 +1295,11 @@ __device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
   const double ilx = 1.0 / Lx, ily = 1.0 / Ly;
   const double ilx_old = 1.0 / Lx_old, ily_old = 1.0 / Ly_old;
   const int items = P.items;
-  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * items + threadIdx.x;
-  const int64_t end = P.p0 + P.n;
+  // a block covers spb slots per pass (kThreads / lanes; the other threads
+  // only join the reduction)
+  const int spb = LN ? kThreads / P.lanes : kThreads;
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * spb * items + threadIdx.x;
+  const int64_t end = (!LN || (int)threadIdx.x < spb) ? P.p0 + P.n : 0;
   DriftCtx dc;
   dc.dt = dt;
   dc.h = h;
@@ -1284,7 +1323,7 @@ __device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
   if (!skip && !boxbad) {
 #pragma unroll 1
     for (int it = 0; it < items; ++it) {
-      const int64_t i = base + (int64_t)it * kThreads;
+      const int64_t i = base + (int64_t)it * spb;
       if (i >= end) break;
       drift_particle<DMd>(D, dc, i, D.pos[i], D.vel[i], D.acc[i], D.type[i], D.sb[i], red[0],
                           mx[0], mx[1], mx[2], bad);
@@ -1346,9 +1385,9 @@ __device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
   system_done_and_signal(D, tin.prior | need);
 }
 
-template <int DMd>
+template <int DMd, bool LN>
 __global__ void __launch_bounds__(kThreads, 4) k_drift(Dev D) {
-  drift_phase<DMd>(D, blockIdx.x);
+  drift_phase<DMd, LN>(D, blockIdx.x);
 }
 
 // ------------------------------------------------------ multi-step kernel --
@@ -1407,7 +1446,7 @@ __device__ __forceinline__ int ld_volatile(const int32_t* p) { return *(const vo
 // (Two blocks per SM: the drift and force phases in one kernel need more
 // than the 64 registers of four, which spilled 270 B; the small systems it
 // serves do not need the occupancy.)
-template <int DMd, int FM>
+template <int DMd, int FM, bool LN>
 __global__ void __launch_bounds__(kThreads, 2)
     k_md_steps(Dev D, cudaGraphConditionalHandle h_more, cudaGraphConditionalHandle h_rebuild) {
   BatchGlobal* bg = D.bg;
@@ -1416,7 +1455,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   int64_t done = 0;
   int rebuild = 0, err = 0;
   while (done < todo) {
-    drift_phase<DMd>(D, blockIdx.x);
+    drift_phase<DMd, LN>(D, blockIdx.x);
     grid_barrier(bg, nb);
     if (ld_volatile(&bg->bar_err)) {
       err = 1;
@@ -1426,7 +1465,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       rebuild = 1;
       break;
     }
-    force_phase<FM, true, false>(D, blockIdx.x);
+    force_phase<FM, true, false, LN>(D, blockIdx.x);
     grid_barrier(bg, nb);
     if (ld_volatile(&bg->bar_err)) {
       err = 1;
@@ -1467,9 +1506,10 @@ __global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
 #pragma unroll
   for (int k = 0; k < kNP; ++k) red[k] = 0.0;
   double mx[3] = {0.0, 0.0, 0.0};
-  const int64_t base = P.p0 + (int64_t)(b - P.b0) * kThreads * P.items + threadIdx.x;
-  for (int it = 0; it < P.items; ++it) {
-    const int64_t i = base + (int64_t)it * kThreads;
+  const int spb = kThreads / P.lanes;
+  const int64_t base = P.p0 + (int64_t)(b - P.b0) * spb * P.items + threadIdx.x;
+  for (int it = 0; it < P.items && (int)threadIdx.x < spb; ++it) {
+    const int64_t i = base + (int64_t)it * spb;
     if (i >= P.p0 + P.n) break;
     const double2 v = D.vel[i];
     const double m = type_mass(P, D.type[i]);

@@ -324,7 +324,7 @@ int Engine::proto_graph(cudaGraphExec_t* exec) {
     cudaGraph_t cg = cases[b];
     if (b == B_ENTER) {
       cudaGraphNode_t nobs, nenter;
-      rc = add_kernel_node(cg, nullptr, 0, force_fn(FM_OBS, true), nblocks_, kThreads, dev_, &nobs);
+      rc = add_kernel_node(cg, nullptr, 0, force_fn(FM_OBS, true, lanes_), nblocks_, kThreads, dev_, &nobs);
       if (rc == MDB_OK) add_proto_kernel(cg, &nobs, (void*)k_proto_enter, &nenter);
       continue;
     }
@@ -339,10 +339,10 @@ int Engine::proto_graph(cudaGraphExec_t* exec) {
       dd.use_cond = 1;
       cudaGraphNode_t nd, nc, nf;
       rc = add_kernel_node(cg, prev ? &prev : nullptr, prev ? 1 : 0,
-                           drift_fn(nph ? DM_NPH : DM_NH), nblocks_, kThreads, dd, &nd);
+                           drift_fn(nph ? DM_NPH : DM_NH, lanes_), nblocks_, kThreads, dd, &nd);
       if (rc == MDB_OK) rc = add_cond_rebuild(cg, nd, hr, &nc);
       if (rc == MDB_OK)
-        rc = add_kernel_node(cg, &nc, 1, force_fn(nph ? FM_NPH : FM_NH, true), nblocks_, kThreads,
+        rc = add_kernel_node(cg, &nc, 1, force_fn(nph ? FM_NPH : FM_NH, true, lanes_), nblocks_, kThreads,
                              dev_, &nf);
       prev = nf;
     }
@@ -351,7 +351,7 @@ int Engine::proto_graph(cudaGraphExec_t* exec) {
     add_cond(body, &nswitch, pa.h_obs, cudaGraphCondTypeIf, 1, &nobs_if, &obs_body);
   if (rc == MDB_OK) {
     cudaGraphNode_t nobs;
-    rc = add_kernel_node(obs_body, nullptr, 0, force_fn(FM_OBS, true), nblocks_, kThreads, dev_,
+    rc = add_kernel_node(obs_body, nullptr, 0, force_fn(FM_OBS, true, lanes_), nblocks_, kThreads, dev_,
                          &nobs);
   }
   if (rc == MDB_OK) add_proto_kernel(body, &nobs_if, (void*)k_proto_step, &nstep);

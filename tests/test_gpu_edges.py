@@ -36,7 +36,9 @@ def test_single_particle(built):
 def test_list_overflow_and_no_lists(built, max_neighbors):
     """max_neighbors 6: most lists overflow and those particles scan their
     stencil; -1: no lists. Forces stay on the FP64 oracle, and a short
-    trajectory on the one computed with full lists."""
+    trajectory on the one computed with full lists (the stencil and the list
+    visit the partners in different orders, so the FP32 sums differ in their
+    last bits; over 50 steps that grows to a few 1e-9)."""
     f, cfg = wl.nve_4096(seed=9)
     Lx, Ly = cfg["box_w_global"], cfg["box_h_global"]
     acc, U, W = mdb.compute_forces(cfg, f, Lx, Ly, max_neighbors=max_neighbors)
@@ -50,7 +52,7 @@ def test_list_overflow_and_no_lists(built, max_neighbors):
     a.sample_collect()
     b.sample_collect()
     d = a.get_host_particles()["pos"] - b.get_host_particles()["pos"]
-    assert np.max(np.abs(d)) < 1e-9
+    assert np.max(np.abs(d)) < 1e-8
 
 
 def test_int32_list_offsets(built):
