@@ -181,12 +181,13 @@ int Engine::build() {
     maxn = std::max<int64_t>(maxn, n);
     P.p0 = p0;
     P.n = n;
-    // MDB_LANES=<1|4> fixes the lanes per slot (tuning aid; 0 = automatic).
+    // MDB_LANES=<1|4> fixes the lanes per slot of MD systems (tuning aid;
+    // 0 = automatic); FIRE systems always have one.
     const char* lanes_env = getenv("MDB_LANES");
     const int lanes_fixed = lanes_env ? atoi(lanes_env) : 0;
-    P.lanes = (lanes_fixed == 1 || lanes_fixed == kLanes)
-                  ? lanes_fixed
-                  : ((sp.kind != K_FIRE && n <= kLanesMaxN) ? kLanes : 1);
+    P.lanes = (sp.kind == K_FIRE) ? 1
+              : (lanes_fixed == 1 || lanes_fixed == kLanes) ? lanes_fixed
+              : (n <= kLanesMaxN ? kLanes : 1);
     const int spb = kThreads / P.lanes;  // slots per block and pass
     P.items = items_fixed > 0
                   ? std::min(items_fixed, kMaxItems)
