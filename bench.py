@@ -138,7 +138,7 @@ def make_workload(name, rank):
 def step_roofline(per_gpu_value, hbm_gbs, p_ord, bytes_per_step=97.0):
     """Whole-step roofline: particle-steps/s on one GPU against
     min(HBM bandwidth / bytes per particle-step, FP32 peak / (24 flops x
-    ordered pairs inside the cutoff per particle)). 97 B is the survey's
+    ordered pairs inside the cutoff per particle)). 97 B is the specified
     algorithmic figure (FP64 pos/vel/force read and written, 1 B type); this
     design moves 173 B (force phase 65 B + drift phase 108 B)."""
     bw_bound = hbm_gbs * 1e9 / bytes_per_step

@@ -1,6 +1,6 @@
 """Force/energy/virial parity of the sm_100a pair kernel against the CPU oracle.
 
-Tolerance: relative force error ||F_gpu - F_fp64|| /
+Tolerance (the accuracy bound): relative force error ||F_gpu - F_fp64|| /
 ||F_fp64|| <= 1e-5 against the FP64 oracle. Energies and virials are FP64
 reductions of FP32 pair terms: relative 1e-6.
 """

@@ -6,7 +6,7 @@ src/md_cuda_common.cu with its host step logic restated at world size 1
 
 * the oracle's reference-arithmetic mode reproduces the reference kernels bit
   for bit at the configurations' sizes (live, beyond the committed fixtures);
-* the product's forces are within the north-star bound (relative L2 1e-5) of
+* the product's forces are within the accuracy bound (relative L2 1e-5) of
   the reference kernel's and closer than them to the FP64 truth;
 * energies, pressure and dU/dlambda agree; the NVE, Nose-Hoover, NPH and
   piston steps track the reference's steps.
