@@ -144,8 +144,25 @@ typedef struct mdb_options {
                              kernels, whose launch costs less);
                              MDB_STEPS_PER_PHASE: one kernel per phase.
                              Both give the same result bits.               */
-  int32_t reserved[8];
+  int32_t lanes;          /* lanes per particle in the force phase of MD
+                             systems of at most 16,384 particles:
+                             MDB_LANES_SPLIT: 4 lanes split each particle's
+                             pair candidates (4x the warps for a small system;
+                             the force sums change in their last bits);
+                             MDB_LANES_ONE: one lane (the order of batches);
+                             MDB_LANES_AUTO (0, default): SPLIT for
+                             single-system simulation handles, ONE for batch,
+                             multi-device and server handles (where a batch
+                             fills the GPU and splitting costs ~30%). A system
+                             gives the same bits alone and in a batch when
+                             both handles use the same setting. FIRE systems
+                             always use one lane.                          */
+  int32_t reserved[7];
 } mdb_options_t;
+
+#define MDB_LANES_AUTO 0
+#define MDB_LANES_ONE 1
+#define MDB_LANES_SPLIT 4
 
 #define MDB_STEPS_AUTO 0
 #define MDB_STEPS_PER_PHASE 1

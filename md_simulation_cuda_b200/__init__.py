@@ -26,7 +26,8 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import (FIRE_AUTO, FIRE_FP32, FIRE_FP64, STEPS_AUTO, STEPS_MULTI, STEPS_PER_PHASE,
+from ._lib import (FIRE_AUTO, FIRE_FP32, FIRE_FP64, LANES_AUTO, LANES_ONE, LANES_SPLIT,
+                   STEPS_AUTO, STEPS_MULTI, STEPS_PER_PHASE,
                    MDB_ERR_ARG, MDBConfigC, MDBError,
                    MDBFireParams, MDBMinimizeResult,
                    MDBNphProtocol, MDBNphRecord, MDBNphResult, MDBObservables, MDBRequest,
@@ -156,12 +157,13 @@ class MDSimulation:
                  step: Optional[int] = None, *, frame=None, device: int = 0,
                  skin: Optional[float] = None, use_graphs: bool = True,
                  state_file: Optional[str] = None, max_neighbors: Optional[int] = None,
-                 autotune: bool = False, step_kernel: Optional[int] = None):
+                 autotune: bool = False, step_kernel: Optional[int] = None,
+                 lanes: Optional[int] = None):
         self.cfg_manager = config_manager if isinstance(config_manager, MDConfigManager) \
             else MDConfigManager(_config_of(config_manager))
         self._h = C.c_void_p()
         opt = options(device, skin, use_graphs, max_neighbors, autotune=autotune,
-                      step_kernel=step_kernel)
+                      step_kernel=step_kernel, lanes=lanes)
         cfg = self.cfg_manager.config
         if state_file is not None:
             # a checkpoint: frame `step` of `filename` plus the integrator state
@@ -532,10 +534,10 @@ class Batch:
 
     def __init__(self, device: int = 0, skin: Optional[float] = None, use_graphs: bool = True,
                  fire_precision: Optional[int] = None, autotune: bool = False,
-                 max_neighbors: Optional[int] = None):
+                 max_neighbors: Optional[int] = None, lanes: Optional[int] = None):
         self._h = C.c_void_p()
         self._opt = options(device, skin, use_graphs, max_neighbors,
-                            fire_precision=fire_precision, autotune=autotune)
+                            fire_precision=fire_precision, autotune=autotune, lanes=lanes)
         check(lib().mdb_batch_create(C.byref(self._opt), C.byref(self._h)))
         self._sizes = []
         self._caps = []

@@ -103,7 +103,8 @@ class MDBOptions(C.Structure):
         ("fire_precision", C.c_int32),
         ("autotune", C.c_int32),
         ("step_kernel", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("lanes", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -403,13 +404,16 @@ def check(rc: int):
 
 FIRE_AUTO, FIRE_FP32, FIRE_FP64 = 0, 1, 2
 STEPS_AUTO, STEPS_PER_PHASE, STEPS_MULTI = 0, 1, 2
+LANES_AUTO, LANES_ONE, LANES_SPLIT = 0, 1, 4
 
 
 def options(device=0, skin=None, use_graphs=True, max_neighbors=None,
-            fire_precision=None, autotune=None, step_kernel=None) -> MDBOptions:
+            fire_precision=None, autotune=None, step_kernel=None, lanes=None) -> MDBOptions:
     o = MDBOptions()
     lib().mdb_options_default(C.byref(o))
     o.device = device
+    if lanes is not None:
+        o.lanes = int(lanes)
     if step_kernel is not None:
         o.step_kernel = int(step_kernel)
     if autotune is not None:

@@ -60,6 +60,8 @@ int sim_make(const mdb_config_t* cfg, std::vector<mdb_particle_t>&& frame,
   if (!sim) return mdb::set_error(MDB_ERR_CAPACITY, "out of host memory");
   sim->cfg = *cfg;
   mdb_options_t o = opts_or_default(opt);
+  // a lone small system splits its pair candidates over four lanes
+  if (o.lanes == MDB_LANES_AUTO) o.lanes = MDB_LANES_SPLIT;
   sim->eng.reset(new Engine(o));
   SystemSpec spec;
   spec.cfg = *cfg;

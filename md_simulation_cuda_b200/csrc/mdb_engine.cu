@@ -76,6 +76,7 @@ Engine::Engine(const mdb_options_t& opt) {
   fire_prec_ = opt.fire_precision;
   autotune_ = opt.autotune;
   step_kernel_ = opt.step_kernel;
+  lanes_opt_ = opt.lanes;
   // MDB_EAGER=1 issues every phase as a separate launch (profilers cannot
   // see kernel nodes of graphs that contain conditional nodes).
   const char* eager = getenv("MDB_EAGER");
@@ -181,13 +182,9 @@ int Engine::build() {
     maxn = std::max<int64_t>(maxn, n);
     P.p0 = p0;
     P.n = n;
-    // MDB_LANES=<1|4> fixes the lanes per slot of MD systems (tuning aid;
-    // 0 = automatic); FIRE systems always have one.
-    const char* lanes_env = getenv("MDB_LANES");
-    const int lanes_fixed = lanes_env ? atoi(lanes_env) : 0;
-    P.lanes = (sp.kind == K_FIRE) ? 1
-              : (lanes_fixed == 1 || lanes_fixed == kLanes) ? lanes_fixed
-              : (n <= kLanesMaxN ? kLanes : 1);
+    // lanes per slot: split for small MD systems when the handle asks for it
+    // (simulation handles resolve MDB_LANES_AUTO to split, batches to one)
+    P.lanes = (sp.kind != K_FIRE && lanes_opt_ == MDB_LANES_SPLIT && n <= kLanesMaxN) ? kLanes : 1;
     const int spb = kThreads / P.lanes;  // slots per block and pass
     P.items = items_fixed > 0
                   ? std::min(items_fixed, kMaxItems)

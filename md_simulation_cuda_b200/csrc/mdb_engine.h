@@ -151,6 +151,7 @@ class Engine {
   int step_kernel_ = MDB_STEPS_AUTO;
   bool multi_step_ = false;
   bool lanes_ = false;  // some system has several lanes per slot (SysParams::lanes)
+  int lanes_opt_ = MDB_LANES_ONE;  // mdb_options_t.lanes (AUTO counts as ONE here)
   int multi_cap_ = 0;  // blocks of the multi-step kernel the device holds at once
   mdb_schedule_t schedule_{};
   int stream_priority_ = 0;  // levels above normal for stream_

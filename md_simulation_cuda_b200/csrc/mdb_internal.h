@@ -34,10 +34,10 @@ constexpr int32_t kListInterior = 1 << 30;
 // Force phase: list rows of the next chunk prefetched into L1 per warp
 // (built-in schedule; Dev::pf_rows holds the one in use).
 constexpr int kListPrefetchRows = 28;
-// Small MD systems (n <= kLanesMaxN) give each slot kLanes lanes of the force
-// phase, which split its pair candidates; a block then covers kThreads /
-// kLanes slots in every phase. A rule on the system alone, so a system gets
-// the same bits alone and in a batch. FIRE systems keep one lane per slot.
+// With mdb_options_t.lanes = MDB_LANES_SPLIT, small MD systems (n <=
+// kLanesMaxN) give each slot kLanes lanes of the force phase, which split its
+// pair candidates; a block then covers kThreads / kLanes slots in every
+// phase. FIRE systems keep one lane per slot.
 constexpr int kLanes = 4;
 constexpr int kLanesMaxN = 16384;
 // MD calls of at least this many steps use the multi-step kernel where it is

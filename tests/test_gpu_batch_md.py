@@ -20,10 +20,15 @@ def _systems():
     return out
 
 
+@pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("nose_hoover", [True, False])
-def test_batch_md_equals_solo(built, nose_hoover):
+def test_batch_md_equals_solo(built, nose_hoover, split):
+    """A system gives the same bits in a batch and alone when both handles
+    use the same lanes setting: one lane (the batch default; the simulation
+    handle asked for it) or split lanes (the simulation default; the batch
+    asked for it)."""
     systems = _systems()
-    b = mdb.Batch()
+    b = mdb.Batch(lanes=mdb.LANES_SPLIT) if split else mdb.Batch()
     kind = mdb.JOB_NVT if nose_hoover else mdb.JOB_NVE
     ids = [b.add_md(cfg, f, kind, nsteps) for f, cfg, nsteps in systems]
     b.run(-1)
@@ -31,7 +36,8 @@ def test_batch_md_equals_solo(built, nose_hoover):
     for sid, (f, cfg, nsteps) in zip(ids, systems):
         n, done, steps = b.system_info(sid)
         assert done and steps == nsteps and n == len(f)
-        sim = mdb.MDSimulation(cfg, frame=f)
+        sim = (mdb.MDSimulation(cfg, frame=f) if split
+               else mdb.MDSimulation(cfg, frame=f, lanes=mdb.LANES_ONE))
         if nose_hoover:
             sim.step_single_nose_hoover(nsteps=nsteps)
         else:

@@ -86,7 +86,8 @@ def test_batch_with_a_single_particle_system(built):
         b.add_md(cfg, f, mdb.JOB_NVE, 80)
     b.run(-1)
     for sid, (f, cfg) in enumerate(systems):
-        sim = mdb.MDSimulation(cfg, frame=f)
+        # the batch's setting: one lane per particle
+        sim = mdb.MDSimulation(cfg, frame=f, lanes=mdb.LANES_ONE)
         sim.step_single_NVE(nsteps=80)
         sim.sample_collect()
         assert np.array_equal(b.frame(sid)["pos"], sim.get_host_particles()["pos"])

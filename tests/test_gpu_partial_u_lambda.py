@@ -56,7 +56,8 @@ def test_partial_U_lambda_batch_equals_solo(built):
         f, Lx, Ly = wl.lattice_frame(1200, 0.8, 1.0, 0.65, T, seed=60 + k, jitter=0.1)
         cfg = wl.config_dict(1200, Lx, Ly, dt=0.002, T=T)
         b.add_md(cfg, f, mdb.JOB_NVT, 100)
-        sim = mdb.MDSimulation(cfg, frame=f)
+        # the batch's setting: one lane per particle
+        sim = mdb.MDSimulation(cfg, frame=f, lanes=mdb.LANES_ONE)
         sim.step_single_nose_hoover(nsteps=100)
         solos.append(sim.cal_partial_U_lambda(EPS))
     b.run(-1)

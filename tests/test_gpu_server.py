@@ -56,7 +56,9 @@ def test_server_results_equal_solo(built):
     for k, (f, cfg, nsteps, nh) in enumerate(md_jobs):
         r = results[("md", k)]
         assert r.steps == nsteps and r.t_submit <= r.t_start <= r.t_done
-        sim = mdb.MDSimulation(cfg, frame=f)
+        # the server's batches use one lane per particle, as a simulation
+        # handle does when asked
+        sim = mdb.MDSimulation(cfg, frame=f, lanes=mdb.LANES_ONE)
         if nh:
             sim.step_single_nose_hoover(nsteps=nsteps)
         else:
