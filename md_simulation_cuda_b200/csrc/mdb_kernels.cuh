@@ -1211,7 +1211,8 @@ __device__ __forceinline__ void drift_particle(const Dev& D, const DriftCtx& c, 
 // k_md_steps: a phase of its multi-step loop).
 template <int DMd, bool LN>
 __device__ __forceinline__ void drift_phase(const Dev& D, const int b) {
-  const int s = D.sys_of_block[b];
+  // (a lone system needs no table lookup: one dependent load less per block)
+  const int s = D.nsys == 1 ? 0 : D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
   {
@@ -1498,7 +1499,8 @@ __global__ void k_md_steps_set(Dev D, int64_t n) {
 // S.K for every system.
 __global__ void __launch_bounds__(kThreads) k_reduce_K(Dev D) {
   const int b = blockIdx.x;
-  const int s = D.sys_of_block[b];
+  // (a lone system needs no table lookup: one dependent load less per block)
+  const int s = D.nsys == 1 ? 0 : D.sys_of_block[b];
   const SysParams& P = D.sp[s];
   SysState* S = D.st + s;
   constexpr int kNS = 1, kNM = 0;
