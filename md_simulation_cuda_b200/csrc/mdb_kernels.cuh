@@ -1803,33 +1803,47 @@ __device__ __forceinline__ int build_list(const Dev& D, const SysParams& P, cons
       r1[1] = D.cstart[row + 1];
       nr = 2;
     }
-    for (int r = 0; r < nr; ++r) {
-      for (int j = r0[r]; j < r1[r]; ++j) {
-        if (j == k) continue;
-        const float4 q = D.pff[j];
-        float2 dd;
-        const float r2 = pair_r2<MIC>(q, c, dd);
-        const float rl2 = (ff_class(q) == ts) ? rl2s : rl2ab;
-        if (r2 < rl2) {
-          int d = j - (int)k;  // offset modulo n into [-n/2, n/2)
-          if (d >= half) {
-            d -= P.n;
-            nowrap = 0;
-          }
-          if (d < -half) {
-            d += P.n;
-            nowrap = 0;
-          }
-          if (D.nl16 && (d > 32767 || d < -32768)) return maxn + 1;  // use the stencil
-          if (cnt < maxn) {
-            if (D.nl16)
-              D.nlist16[(int64_t)cnt * D.ntot + k] = (int16_t)d;
-            else
-              D.nlist[(int64_t)cnt * D.ntot + k] = d;
-          }
-          ++cnt;
+    // visit(j, q): false when the list must give up (16-bit offsets overflow)
+    auto visit = [&](int j, const float4 q) -> bool {
+      if (j == k) return true;
+      float2 dd;
+      const float r2 = pair_r2<MIC>(q, c, dd);
+      const float rl2 = (ff_class(q) == ts) ? rl2s : rl2ab;
+      if (r2 < rl2) {
+        int d = j - (int)k;  // offset modulo n into [-n/2, n/2)
+        if (d >= half) {
+          d -= P.n;
+          nowrap = 0;
         }
+        if (d < -half) {
+          d += P.n;
+          nowrap = 0;
+        }
+        if (D.nl16 && (d > 32767 || d < -32768)) return false;
+        if (cnt < maxn) {
+          if (D.nl16)
+            D.nlist16[(int64_t)cnt * D.ntot + k] = (int16_t)d;
+          else
+            D.nlist[(int64_t)cnt * D.ntot + k] = d;
+        }
+        ++cnt;
       }
+      return true;
+    };
+    for (int r = 0; r < nr; ++r) {
+      int j = r0[r];
+      const int je = r1[r];
+      // four candidates' positions in flight at a time
+      for (; j + 4 <= je; j += 4) {
+        float4 qq[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) qq[u] = D.pff[j + u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (!visit(j + u, qq[u])) return maxn + 1;  // use the stencil
+      }
+      for (; j < je; ++j)
+        if (!visit(j, D.pff[j])) return maxn + 1;
     }
   }
   return cnt;
