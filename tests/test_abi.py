@@ -107,3 +107,45 @@ def test_server_option_defaults_and_checks(built):
     e = _lib.MDBOptions()
     _lib.lib().mdb_options_default(C.byref(e))
     assert e.skin == 0.0 and e.stream_priority == 0 and e.max_neighbors == 48
+
+
+# ctypes mirror -> C typedef of include/mdb200.h
+_MIRRORS = {
+    "MDBConfigC": "mdb_config_t", "MDBOptions": "mdb_options_t",
+    "MDBSchedule": "mdb_schedule_t", "MDBObservables": "mdb_observables_t",
+    "MDBFireParams": "mdb_fire_params_t", "MDBMinimizeResult": "mdb_minimize_result_t",
+    "MDBServerOptions": "mdb_server_options_t", "MDBRequest": "mdb_request_t",
+    "MDBRequestResult": "mdb_request_result_t", "MDBServerStats": "mdb_server_stats_t",
+    "MDBNphProtocol": "mdb_nph_protocol_t", "MDBNphRecord": "mdb_nph_record_t",
+    "MDBNphResult": "mdb_nph_result_t",
+}
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every ctypes mirror has the size and field offsets that a C compiler
+    gives the header's struct (a C program compiled against
+    include/mdb200.h prints them)."""
+    import subprocess
+
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "mdb200.h"',
+             "int main(void) {"]
+    for py, c in _MIRRORS.items():
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in getattr(_lib, py)._fields_:
+            lines.append(f'  printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-I",
+                    "/usr/local/cuda/include", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {}
+    for line in out.splitlines():
+        py, key, val = line.split()
+        got[(py, key)] = int(val)
+    for py in _MIRRORS:
+        cls = getattr(_lib, py)
+        assert got[(py, "size")] == C.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert got[(py, name)] == getattr(cls, name).offset, (py, name)
