@@ -144,3 +144,25 @@ def test_protocol_from_config(built):
     assert q.auto_target == 1  # pressure_target_mode defaults to "auto_initial"
     assert q.eval_interval == 50 and q.production_steps == 1234
     assert q.window_samples == 50 and q.tolerance_rel == 0.05
+
+
+@pytest.mark.parametrize("kw", [
+    dict(eval_interval=1, window_samples=1, stable_required=1),       # every step sampled, clamps
+    dict(auto_steps=1, warmup_min_steps=0, warmup_max_steps=1),      # shortest phases
+    dict(warmup_min_steps=500, warmup_max_steps=100),                # max below min: clamped
+    dict(eval_interval=7, window_samples=3, stable_required=2, production_steps=1),
+    dict(eval_interval=0, auto_steps=0, stable_required=0, production_steps=0),  # zeros: clamped
+])
+def test_protocol_edge_parameters(built, kw):
+    """Degenerate and clamped parameters take the same decisions chunked as in
+    the per-step loop."""
+    p = scripts()["settle"]
+    q = protocol(**kw)
+    ref = literal(q, p)
+    res, recs, _ = mdb.nph_protocol_dry_run(q, p)
+    assert (res.P_target, res.auto_end_step, res.warmup_end_step, bool(res.forced_switch),
+            bool(res.finished), res.total_steps) == (
+        ref["P_target"], ref["auto_end"], ref["warm_end"], ref["forced"], ref["finished"],
+        ref["total"])
+    got = [(r.step, r.phase, r.P_inst, r.P_target, r.mean, r.stddev) for r in recs]
+    assert got == ref["recs"]
