@@ -149,3 +149,42 @@ def test_ctypes_structs_match_the_header(tmp_path):
         assert got[(py, "size")] == C.sizeof(cls), py
         for name, _ in cls._fields_:
             assert got[(py, name)] == getattr(cls, name).offset, (py, name)
+
+
+_NULL_CALLS = r"""
+import ctypes as C, json, sys
+from md_simulation_cuda_b200 import _lib
+L = _lib.lib()
+out = {}
+for name, (argt, res) in sorted(_lib.SIGNATURES.items()):
+    args = [0.0 if a is C.c_double else 0 if a in (C.c_int, C.c_int32, C.c_int64, C.c_long,
+            C.c_ulong, C.c_size_t) else None for a in argt]
+    rc = getattr(L, name)(*args)
+    out[name] = rc if isinstance(rc, int) or rc is None else repr(rc)
+print(json.dumps(out))
+"""
+
+
+def test_null_arguments_return_a_status(built):
+    """Every entry point called with null pointers and zero sizes returns a
+    status instead of crashing: MDB_ERR_ARG, except the destroy/close calls
+    (no-ops on a null handle, as free(NULL)) and the three getters without a
+    status. Runs in a child process so that a crash fails the test."""
+    import json
+    import subprocess
+    import sys
+
+    env = dict(os.environ, PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    p = subprocess.run([sys.executable, "-c", _NULL_CALLS], capture_output=True, text=True,
+                       env=env, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    got = json.loads(p.stdout.strip().splitlines()[-1])
+    assert set(got) == set(_lib.SIGNATURES)
+    noop = {n for n in got if n.endswith(("_destroy", "_close"))}
+    no_status = {"mdb_kernel_launches", "mdb_version", "mdb_options_default",
+                 "mdb_server_options_default"}
+    for name, rc in got.items():
+        if name in noop:
+            assert rc == 0, name
+        elif name not in no_status:
+            assert rc == _lib.MDB_ERR_ARG, (name, rc)
