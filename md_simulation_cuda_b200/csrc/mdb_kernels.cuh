@@ -1407,7 +1407,12 @@ constexpr unsigned kBarrierSpins = 1u << 22;
 // Grid-wide barrier. Thread 0 of each block arrives on a counter; the last
 // arrival resets it and advances the generation (release), the others poll
 // the generation (acquire). A wait that runs out of polls records bar_err
-// and returns; the kernel stops at its next check.
+// and returns; the kernel stops at its next check. That error is final for
+// the handle: the kernel sets the system's err flag, after which every phase
+// skips the system and every call reports it. Each call clears the arrival
+// counter before its first launch (k_md_steps_set), so that a later call on
+// such a handle passes its barriers and stops at once instead of waiting out
+// the polls on arrivals that an abandoned barrier left behind.
 __device__ __forceinline__ void grid_barrier(BatchGlobal* bg, unsigned nblocks) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1492,7 +1497,10 @@ __global__ void k_md_steps_count(Dev D, cudaGraphConditionalHandle h_more) {
 }
 
 __global__ void k_md_steps_set(Dev D, int64_t n) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) D.bg->steps_left = n;
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    D.bg->steps_left = n;
+    D.bg->bar_count = 0u;  // no multi-step block runs now (stream order)
+  }
 }
 
 // K = sum 1/2 m |v|^2 (cal_local_K_kernel src/md_cuda_common.cu:554-589) into
